@@ -1,0 +1,215 @@
+// Explicit 4-stage Runge-Kutta pseudo-time stepping with local time steps and
+// implicit residual smoothing, the fallback solver of aero2d/euler.py:289-346.
+//
+// Smoothing along i (periodic, constant coefficients -e, 1+2e, -e) is the
+// exact solution of the circulant system, which the reference obtains by FFT
+// (euler.py:302-303).  Here it is applied through the system's periodic Green's
+// function g_m = G0 (l^m + l^(n-m)) / (1 - l^n), l the root in (0,1) of
+// e l^2 - (1+2e) l + e = 0 and G0 = 1 / (e (1/l - l)); terms with l^|m| below
+// 1e-18 of the diagonal are dropped, so results equal the FFT's to rounding.
+// Smoothing along j is a Thomas solve of (-e, 1+2e, -e) with end diagonals 1+e.
+#include "batch.cuh"
+#include "explicit.cuh"
+#include "physics.cuh"
+
+namespace a2d {
+
+// local time step dt = cfl vol / (lambda_i + lambda_j)   (euler.py:289-296)
+__global__ void __launch_bounds__(256) k_local_dt(Batch b, const double* __restrict__ U, double* __restrict__ dt,
+                                                  double cfl) {
+  const Tile t = b.tiles[blockIdx.x];
+  const CaseDev& cs = b.cases[t.cs];
+  const GridDev& g = cs.g;
+  const int ni = g.ni, nc = g.nc;
+  const size_t N = (size_t)ni * nc, NJ = (size_t)(nc + 1) * ni;
+  const double* Uc = U + 4 * cs.cell_off;
+  for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
+    const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
+    const int ip = (i + 1 == ni) ? 0 : i + 1;
+    State4<double> u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) u.c[k] = Uc[vidx(g, k, j, i)];
+    const State4<double> W = cons_to_prim<double, double>(u);
+    const double cc = sqrt(kGamma * W.c[3] / W.c[0]);
+    const double s0 = 0.5 * (g.Si[(size_t)j * ni + i] + g.Si[(size_t)j * ni + ip]);
+    const double s1 = 0.5 * (g.Si[N + (size_t)j * ni + i] + g.Si[N + (size_t)j * ni + ip]);
+    const double t0 = 0.5 * (g.Sj[(size_t)(j + 1) * ni + i] + g.Sj[(size_t)j * ni + i]);
+    const double t1 = 0.5 * (g.Sj[NJ + (size_t)(j + 1) * ni + i] + g.Sj[NJ + (size_t)j * ni + i]);
+    const double li = fabs(W.c[1] * s0 + W.c[2] * s1) + cc * sqrt(s0 * s0 + s1 * s1);
+    const double lj = fabs(W.c[1] * t0 + W.c[2] * t1) + cc * sqrt(t0 * t0 + t1 * t1);
+    dt[cs.cell_off + (size_t)j * ni + i] = cfl * g.vol[(size_t)j * ni + i] / (li + lj);
+  }
+}
+
+// periodic smoothing along i: one block per (case, component, row j)
+__global__ void __launch_bounds__(256) k_irs_i(Batch b, const double* __restrict__ R, double* __restrict__ out,
+                                               double e) {
+  const int row = blockIdx.x;   // rows enumerated as (case, k, j) via the row table below
+  const int cs_id = blockIdx.y;
+  const CaseDev& cs = b.cases[cs_id];
+  const GridDev& g = cs.g;
+  const int ni = g.ni, nc = g.nc;
+  if (row >= 4 * nc) return;
+  const int k = row / nc, j = row % nc;
+  extern __shared__ double sm[];
+  double* r = sm;          // ni
+  double* gm = sm + ni;    // up to ni/2 + 1
+  const double* src = R + 4 * cs.cell_off + vidx(g, k, j, 0);
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) r[i] = src[i];
+  const double lam = ((1.0 + 2.0 * e) - sqrt(1.0 + 4.0 * e)) / (2.0 * e);
+  const double G0 = 1.0 / (e * (1.0 / lam - lam));
+  int M = (int)ceil(log(1e-18) / log(lam));
+  if (M > ni / 2) M = ni / 2;
+  const double ln = pow(lam, (double)ni);
+  for (int m = threadIdx.x; m <= M; m += blockDim.x)
+    gm[m] = G0 * (pow(lam, (double)m) + pow(lam, (double)(ni - m))) / (1.0 - ln);
+  __syncthreads();
+  double* dst = out + 4 * cs.cell_off + vidx(g, k, j, 0);
+  const bool full = (2 * M + 1 >= ni);
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+    double s = gm[0] * r[i];
+    if (full) {
+      for (int d = 1; d < ni; ++d) {
+        const int m = d <= ni / 2 ? d : ni - d;
+        int q = i - d;
+        if (q < 0) q += ni;
+        s += gm[m] * r[q];
+      }
+    } else {
+      for (int m = 1; m <= M; ++m) {
+        int qm = i - m, qp = i + m;
+        if (qm < 0) qm += ni;
+        if (qp >= ni) qp -= ni;
+        s += gm[m] * (r[qm] + r[qp]);
+      }
+    }
+    dst[i] = s;
+  }
+}
+
+// smoothing along j: Thomas solve per (case, component, line i); thread per line.
+// The elimination coefficients depend on j only and are formed once per block.
+__global__ void __launch_bounds__(128) k_irs_j(Batch b, double* __restrict__ R, double e) {
+  const int cs_id = blockIdx.y;
+  const CaseDev& cs = b.cases[cs_id];
+  const GridDev& g = cs.g;
+  const int ni = g.ni, nc = g.nc;
+  extern __shared__ double cpj[];   // nc
+  if (threadIdx.x == 0) {
+    double cp = 0.0;
+    for (int j = 0; j < nc; ++j) {
+      const double dj = (j == 0 || j == nc - 1) ? 1.0 + e : 1.0 + 2.0 * e;
+      const double lj = (j == 0) ? 0.0 : -e;
+      const double uj = (j == nc - 1) ? 0.0 : -e;
+      cp = uj / (dj - lj * cp);
+      cpj[j] = cp;
+    }
+  }
+  __syncthreads();
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= 4 * ni) return;
+  const int k = line / ni, i = line % ni;
+  double* x = R + 4 * cs.cell_off;
+  double dprev = 0.0;
+  for (int j = 0; j < nc; ++j) {
+    const double dj = (j == 0 || j == nc - 1) ? 1.0 + e : 1.0 + 2.0 * e;
+    const double lj = (j == 0) ? 0.0 : -e;
+    const double den = dj - lj * (j == 0 ? 0.0 : cpj[j - 1]);
+    const double v = (x[vidx(g, k, j, i)] - lj * dprev) / den;
+    x[vidx(g, k, j, i)] = v;
+    dprev = v;
+  }
+  double xn = 0.0;
+  for (int j = nc - 1; j >= 0; --j) {
+    const double v = x[vidx(g, k, j, i)] - cpj[j] * xn;
+    x[vidx(g, k, j, i)] = v;
+    xn = v;
+  }
+}
+
+// U = U0 - a (dt / vol) R   (euler.py:344)
+__global__ void __launch_bounds__(256) k_rk_stage(Batch b, const double* __restrict__ U0,
+                                                  const double* __restrict__ R, const double* __restrict__ dt,
+                                                  double* __restrict__ U, double a) {
+  const Tile t = b.tiles[blockIdx.x];
+  const CaseDev& cs = b.cases[t.cs];
+  const GridDev& g = cs.g;
+  const size_t base = 4 * cs.cell_off;
+  for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
+    const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
+    const size_t cell = (size_t)j * g.ni + i;
+    const double f = a * (dt[cs.cell_off + cell] / g.vol[cell]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const size_t q = base + vidx(g, k, j, i);
+      U[q] = U0[q] - f * R[q];
+    }
+  }
+}
+
+// per-tile sum of ((U_rho - U0_rho) / dt)^2
+__global__ void __launch_bounds__(256) k_rk_res(Batch b, const double* __restrict__ U0,
+                                                const double* __restrict__ U, const double* __restrict__ dt,
+                                                double* __restrict__ tpart) {
+  const Tile t = b.tiles[blockIdx.x];
+  const CaseDev& cs = b.cases[t.cs];
+  const GridDev& g = cs.g;
+  const size_t base = 4 * cs.cell_off;
+  double s = 0.0;
+  for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
+    const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
+    const size_t q = base + vidx(g, 0, j, i);
+    const double r = (U[q] - U0[q]) / dt[cs.cell_off + (size_t)j * g.ni + i];
+    s += r * r;
+  }
+  __shared__ double sc[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) sc[w] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) tot += sc[q];
+    tpart[(size_t)blockIdx.x * kTilePartStride + 3] = tot;
+  }
+}
+
+// res = sqrt(mean(...)) per case; circ = 1/2 Cl M from the forces   (euler.py:345, :401-403)
+__global__ void k_rk_finish(Batch b, const double* tpart, const double* coef, double* res, double* circ) {
+  const int cs = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cs >= b.ncases) return;
+  const CaseDev& c = b.cases[cs];
+  double s = 0.0;
+  for (int q = 0; q < c.ntiles; ++q) s += tpart[(size_t)(c.tile0 + q) * kTilePartStride + 3];
+  const double N = (double)c.g.ni * (double)c.g.nc;
+  if (res != nullptr) res[cs] = sqrt(s / N);
+  const double mach = sqrt(c.winf[1] * c.winf[1] + c.winf[2] * c.winf[2]);
+  circ[cs] = 0.5 * coef[3 * cs] * mach;
+}
+
+void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, cudaStream_t s) {
+  if (b.ntiles) k_local_dt<<<b.ntiles, 256, 0, s>>>(b, U, dt, cfl);
+}
+void launch_irs(const Batch& b, double* R, double* tmp, double e, int max_ni, int max_nc, cudaStream_t s) {
+  if (e <= 0.0 || b.ncases == 0) return;
+  dim3 gi(4 * max_nc, b.ncases);
+  const size_t sm = (size_t)(max_ni + max_ni / 2 + 2) * sizeof(double);
+  k_irs_i<<<gi, 256, sm, s>>>(b, R, tmp, e);
+  dim3 gj((4 * max_ni + 127) / 128, b.ncases);
+  k_irs_j<<<gj, 128, (size_t)max_nc * sizeof(double), s>>>(b, tmp, e);
+}
+void launch_rk_stage(const Batch& b, const double* U0, const double* R, const double* dt, double* U, double a,
+                     cudaStream_t s) {
+  if (b.ntiles) k_rk_stage<<<b.ntiles, 256, 0, s>>>(b, U0, R, dt, U, a);
+}
+void launch_rk_res(const Batch& b, const double* U0, const double* U, const double* dt, double* tpart,
+                   cudaStream_t s) {
+  if (b.ntiles) k_rk_res<<<b.ntiles, 256, 0, s>>>(b, U0, U, dt, tpart);
+}
+void launch_rk_finish(const Batch& b, const double* tpart, const double* coef, double* res, double* circ,
+                      cudaStream_t s) {
+  k_rk_finish<<<(b.ncases + 63) / 64, 64, 0, s>>>(b, tpart, coef, res, circ);
+}
+
+}  // namespace a2d

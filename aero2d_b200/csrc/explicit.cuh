@@ -1,0 +1,19 @@
+// Launchers of the explicit RK4 + residual-smoothing kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "batch.cuh"
+
+namespace a2d {
+
+void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, cudaStream_t s);
+// R (in) -> tmp (out, smoothed along i then j)
+void launch_irs(const Batch& b, double* R, double* tmp, double e, int max_ni, int max_nc, cudaStream_t s);
+void launch_rk_stage(const Batch& b, const double* U0, const double* R, const double* dt, double* U, double a,
+                     cudaStream_t s);
+void launch_rk_res(const Batch& b, const double* U0, const double* U, const double* dt, double* tpart,
+                   cudaStream_t s);
+void launch_rk_finish(const Batch& b, const double* tpart, const double* coef, double* res, double* circ,
+                      cudaStream_t s);
+
+}  // namespace a2d

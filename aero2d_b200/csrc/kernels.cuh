@@ -1,0 +1,82 @@
+// Launcher declarations and argument blocks of the Euler-path kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "batch.cuh"
+
+namespace a2d {
+
+template <typename VT>
+struct StencilArgs {
+  const double* U = nullptr;       // conserved state (FP64), packed cell vectors
+  const VT* V = nullptr;           // tangent direction (linearised mode)
+  const double* circ_in = nullptr; // per-case circulation; nullptr: Gamma(U) from the wall rows
+  const double* diag = nullptr;    // per-cell vol / dtau (linearised mode; nullptr: J v alone)
+  const double* bvec = nullptr;    // linearised mode: out = b - (diag v + J v) when set
+  double* out = nullptr;
+  double sign = 1.0;               // residual mode: out = sign * R
+  double* circ_out = nullptr;      // residual mode: per-case circulation used
+  double* tile_part = nullptr;     // residual mode: per-tile sum of (R_rho / vol)^2
+  double lim_k = 0.02;
+  int order = 2;
+  int vortex = 1;
+  uint32_t need = 0;               // status bits a case needs to be processed
+};
+
+struct JacArgs {
+  const double* U = nullptr;
+  const double* circ = nullptr;    // per-case circulation (held fixed in the far-field block)
+  void* JIL = nullptr;             // i-face blocks dF/dU_left  [rows nc]
+  void* JIR = nullptr;             // i-face blocks dF/dU_right [rows nc]
+  void* JJL = nullptr;             // j-face blocks dF/dU_low   [rows nc+1] (row nc: far field)
+  void* JJR = nullptr;             // j-face blocks dF/dU_high  [rows nc+1] (row 0: wall)
+  int vortex = 1;
+  uint32_t need = 0;
+};
+
+struct FactorArgs {
+  const double* U = nullptr;
+  const CaseCtl* ctl = nullptr;    // per-case pseudo-time CFL
+  const void* JIL = nullptr;
+  const void* JIR = nullptr;
+  const void* JJL = nullptr;
+  const void* JJR = nullptr;
+  double* INV = nullptr;           // inverse of the block-Thomas pivots [rows nc]
+  double* CF = nullptr;            // upper factors c_j                 [rows nc]
+  double* diag = nullptr;          // per-cell vol / dtau
+  double cfl_base = 2.5;           // EulerSolver.cfl, which local_dt multiplies and step() divides out
+  uint32_t need = 0;
+};
+
+struct SweepArgs {
+  const double* r = nullptr;       // right-hand side
+  const double* xprev = nullptr;   // previous sweep (nullptr on the first sweep)
+  double* out = nullptr;
+  const double* INV = nullptr;
+  const double* CF = nullptr;
+  const void* JJL = nullptr;
+  const void* JIL = nullptr;
+  const void* JIR = nullptr;
+  uint32_t need = 0;
+};
+
+void launch_metrics(int ni, int nc, const double* x, const double* y, double* md, float* mf,
+                    cudaStream_t s);
+
+template <typename T, bool LIN, typename VT>
+void launch_stencil(const Batch& b, const StencilArgs<VT>& a, cudaStream_t s);
+
+void launch_forces(const Batch& b, const double* U, double* coef, double* cp, const long long* cp_off,
+                   const CaseCtl* ctl, double* hist_cl, int hist_cap, cudaStream_t s);
+
+template <typename T>
+void launch_face_jac(const Batch& b, const JacArgs& a, cudaStream_t s);
+
+template <typename TJ>
+void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s);
+
+template <typename TJ>
+void launch_sweep(const Batch& b, const SweepArgs& a, cudaStream_t s);
+
+}  // namespace a2d

@@ -1,0 +1,89 @@
+// Argument blocks and launchers of the GMRES / Newton-update kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "batch.cuh"
+
+namespace a2d {
+
+struct CtlParams {
+  double cfl0 = 10.0;
+  double cfl_max = 300.0;
+  double tol = 1e-8;
+  int retire = 1;
+};
+
+template <typename TB>
+struct DotArgs {
+  const double* w = nullptr;
+  const TB* V = nullptr;
+  size_t vstride = 0;      // entries between consecutive basis vectors
+  int nq = 0;              // number of basis vectors
+  int with_norm = 0;       // also w.w in slot nq
+  double* part = nullptr;  // [chunk][pstride]
+  int pstride = 0;
+  uint32_t need = 0;
+};
+
+template <typename TB>
+struct UpdateArgs {
+  double* w = nullptr;
+  const TB* V = nullptr;
+  size_t vstride = 0;
+  int nq = 0;
+  const double* part = nullptr;  // dot partials to reduce
+  int pstride = 0;
+  double* hstore = nullptr;      // [case][kMaxRestart+1] reduced coefficients
+  double* wn0 = nullptr;         // if set: sqrt of slot nq stored per case (norm before orthogonalisation)
+  double* part_norm = nullptr;   // if set: per-chunk squared norm of the updated w
+  uint32_t need = 0;
+};
+
+template <typename TB>
+struct NormalizeArgs {
+  const double* w = nullptr;
+  TB* Vout = nullptr;
+  const double* part_norm = nullptr;
+  const double* wn0 = nullptr;
+  const double* h1 = nullptr;
+  const double* h2 = nullptr;
+  double* H = nullptr;            // [case][kMaxRestart][kMaxRestart+1], column k = step k
+  CaseCtl* ctl = nullptr;
+  uint32_t* live = nullptr;
+  int k = -1;                     // -1: start vector
+  uint32_t need = 0;
+};
+
+template <typename TB>
+struct CombineArgs {
+  const double* x0 = nullptr;
+  const TB* V = nullptr;
+  size_t vstride = 0;
+  const double* y = nullptr;
+  const CaseCtl* ctl = nullptr;
+  double* out = nullptr;
+  uint32_t need = 0;
+};
+
+template <typename TB> void launch_dots(const Batch& b, const DotArgs<TB>& a, cudaStream_t s);
+template <typename TB> void launch_update(const Batch& b, const UpdateArgs<TB>& a, cudaStream_t s);
+template <typename TB> void launch_normalize(const Batch& b, const NormalizeArgs<TB>& a, cudaStream_t s);
+template <typename TB> void launch_combine(const Batch& b, const CombineArgs<TB>& a, cudaStream_t s);
+void launch_lstsq(const Batch& b, const uint32_t* live, CaseCtl* ctl, double* H, double* y, double* scr,
+                  cudaStream_t s);
+void launch_gm_setup(const Batch& b, const double* part, int pstride, CaseCtl* ctl, double gtol,
+                     cudaStream_t s);
+void launch_norms2(const Batch& b, const double* x, const double* y, double* part, int pstride,
+                   uint32_t need, cudaStream_t s);
+void launch_norm1(const Batch& b, const double* x, double* part, uint32_t need, cudaStream_t s);
+void launch_update_rel(const Batch& b, const double* U, const double* dU, double* tpart, uint32_t need,
+                       cudaStream_t s);
+void launch_update_check(const Batch& b, const double* U, const double* dU, double* tpart, CaseCtl* ctl,
+                         double max_update, uint32_t need, cudaStream_t s);
+void launch_controller(const Batch& b, const double* tpart, CaseCtl* ctl, uint32_t* live, double* hist_rn,
+                       int hist_cap, const CtlParams& p, cudaStream_t s);
+void launch_commit(const Batch& b, double* U, const double* dU, const CaseCtl* ctl, cudaStream_t s);
+void launch_mark_stepped(const Batch& b, const uint32_t* live, CaseCtl* ctl, cudaStream_t s);
+
+}  // namespace a2d

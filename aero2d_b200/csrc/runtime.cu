@@ -1,0 +1,930 @@
+// Host runtime of the Euler path: batch plans, workspace layout, the
+// pseudo-transient Newton step as a sequence of kernels (replayed as one CUDA
+// graph), the explicit RK iteration, and the extern "C" entry points declared
+// in include/aero2d_b200.h.
+//
+// A plan owns no device memory: every device array lives in the caller's
+// workspace, carved at bind time.  The Newton loop's per-case bookkeeping
+// (rollback, freeze, SER CFL, convergence test, aero2d/implicit.py:216-244)
+// runs on the device, so the host synchronises once per step only to learn
+// whether any case is still live.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "aero2d_b200.h"
+#include "batch.cuh"
+#include "explicit.cuh"
+#include "kernels.cuh"
+#include "krylov.cuh"
+#include "physics.cuh"
+
+namespace a2d {
+
+thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define A2D_CK(call)                                                                   \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(A2D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+  } while (0)
+
+struct Carve {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    off = (off + 255) & ~size_t(255);
+    const size_t o = off;
+    off += bytes;
+    return o;
+  }
+};
+
+static size_t metrics_doubles(int ni, int nc) {
+  const size_t N = (size_t)ni * nc;
+  return 5 * N + 6 * (size_t)ni;
+}
+static size_t metrics_floats(int ni, int nc) {
+  const size_t N = (size_t)ni * nc;
+  return 5 * N + 4 * (size_t)ni;
+}
+static size_t metrics_total_bytes(int ni, int nc) {
+  return ((metrics_doubles(ni, nc) * 8 + 255) & ~size_t(255)) + metrics_floats(ni, nc) * 4;
+}
+
+static GridDev grid_view(const void* blob, int ni, int nc) {
+  GridDev g;
+  g.ni = ni;
+  g.nc = nc;
+  const size_t N = (size_t)ni * nc;
+  const double* d = static_cast<const double*>(blob);
+  g.vol = d;
+  g.Si = d + N;
+  g.Sj = g.Si + 2 * N;
+  g.xf = g.Sj + 2 * (N + ni);
+  g.yf = g.xf + ni;
+  g.xw = g.yf + ni;
+  g.yw = g.xw + ni;
+  const float* f = reinterpret_cast<const float*>(static_cast<const char*>(blob) +
+                                                  ((metrics_doubles(ni, nc) * 8 + 255) & ~size_t(255)));
+  g.vol_f = f;
+  g.Si_f = f + N;
+  g.Sj_f = g.Si_f + 2 * N;
+  g.xf_f = g.Sj_f + 2 * (N + ni);
+  g.yf_f = g.xf_f + ni;
+  return g;
+}
+
+enum VecSlot { kU = 0, kR, kVin, kJV, kDU, kB, kX0, kT, kRr, kZ, kW, kPA, kPB, kU0, kNumVec };
+
+}  // namespace a2d
+
+using namespace a2d;
+
+struct a2d_plan {
+  a2d_params p{};
+  int ncases = 0;
+  int m = 0;               // GMRES restart
+  int max_ni = 0, max_nc = 0;
+  std::vector<CaseDev> cases;
+  std::vector<Tile> tiles;
+  std::vector<Chunk> chunks;
+  std::vector<Group> groups;
+  std::vector<long long> cp_off;
+  long long C = 0, rows_nc = 0, rows_nc1 = 0, total_ni = 0;
+  size_t tj = 8, tb = 8;   // bytes of face-Jacobian and basis storage entries
+  // workspace layout (offsets)
+  size_t o_cases = 0, o_tiles = 0, o_chunks = 0, o_groups = 0, o_cpoff = 0, o_live = 0, o_ctl = 0;
+  size_t o_vec[kNumVec] = {};
+  size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_V = 0;
+  size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_y = 0, o_lsq = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
+  size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0;
+  int pstride = 0;
+  size_t bytes = 0;
+  char* ws = nullptr;
+  Batch batch{};
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  int* host_count = nullptr;
+  int steps_taken = 0;
+
+  template <typename X> X* at(size_t off) const { return reinterpret_cast<X*>(ws + off); }
+  double* vec(int s) const { return at<double>(o_vec[s]); }
+  CaseCtl* ctl() const { return at<CaseCtl>(o_ctl); }
+  uint32_t* live() const { return at<uint32_t>(o_live); }
+};
+
+namespace a2d {
+
+// ---------------------------------------------------------------------------
+// plan construction
+// ---------------------------------------------------------------------------
+static void build_tables(a2d_plan* P, const int* ni, const int* nc, const void* const* metrics,
+                         const double* winf) {
+  long long cell = 0, rnc = 0, rnc1 = 0, cpo = 0;
+  for (int k = 0; k < P->ncases; ++k) {
+    CaseDev c{};
+    c.g = grid_view(metrics[k], ni[k], nc[k]);
+    for (int q = 0; q < 4; ++q) c.winf[q] = winf[4 * k + q];
+    c.cell_off = cell;
+    c.rows_nc = rnc;
+    c.rows_nc1 = rnc1;
+    const int ngr = (ni[k] + kLanes - 1) / kLanes;
+    c.tile0 = (int)P->tiles.size();
+    for (int j0 = 0; j0 < nc[k]; j0 += kTJ)
+      for (int i0 = 0; i0 < ni[k]; i0 += kTI)
+        P->tiles.push_back(Tile{k, i0, j0, std::min(kTI, ni[k] - i0), std::min(kTJ, nc[k] - j0)});
+    c.ntiles = (int)P->tiles.size() - c.tile0;
+    const long long n4 = 4LL * ni[k] * nc[k];
+    c.chunk0 = (int)P->chunks.size();
+    for (long long b0 = 0; b0 < n4; b0 += kChunk)
+      P->chunks.push_back(Chunk{k, (int)b0, (int)std::min<long long>(kChunk, n4 - b0)});
+    c.nchunks = (int)P->chunks.size() - c.chunk0;
+    c.group0 = (int)P->groups.size();
+    for (int g = 0; g < ngr; ++g)
+      P->groups.push_back(Group{k, g, g * kLanes, std::min(kLanes, ni[k] - g * kLanes)});
+    c.ngroups = ngr;
+    P->cases.push_back(c);
+    P->cp_off.push_back(cpo);
+    cell += (long long)ni[k] * nc[k];
+    rnc += (long long)ngr * nc[k];
+    rnc1 += (long long)ngr * (nc[k] + 1);
+    cpo += ni[k];
+    P->max_ni = std::max(P->max_ni, ni[k]);
+    P->max_nc = std::max(P->max_nc, nc[k]);
+  }
+  P->C = cell;
+  P->rows_nc = rnc;
+  P->rows_nc1 = rnc1;
+  P->total_ni = cpo;
+}
+
+static void layout(a2d_plan* P) {
+  Carve cv;
+  const int B = P->ncases;
+  const size_t C = (size_t)P->C;
+  P->o_cases = cv.take(sizeof(CaseDev) * B);
+  P->o_tiles = cv.take(sizeof(Tile) * P->tiles.size());
+  P->o_chunks = cv.take(sizeof(Chunk) * P->chunks.size());
+  P->o_groups = cv.take(sizeof(Group) * P->groups.size());
+  P->o_cpoff = cv.take(sizeof(long long) * B);
+  P->o_live = cv.take(sizeof(uint32_t) * B);
+  P->o_ctl = cv.take(sizeof(CaseCtl) * B);
+  for (int s = 0; s < kNumVec; ++s) P->o_vec[s] = cv.take(8 * 4 * C);
+  P->o_diag = cv.take(8 * C);
+  P->o_dt = cv.take(8 * C);
+  const size_t lb = (size_t)16 * kLanes;
+  P->o_JIL = cv.take(P->tj * lb * P->rows_nc);
+  P->o_JIR = cv.take(P->tj * lb * P->rows_nc);
+  P->o_JJL = cv.take(P->tj * lb * P->rows_nc1);
+  P->o_JJR = cv.take(P->tj * lb * P->rows_nc1);
+  P->o_INV = cv.take(8 * lb * P->rows_nc);
+  P->o_CF = cv.take(8 * lb * P->rows_nc);
+  P->o_V = cv.take(P->tb * 4 * C * (size_t)(P->m + 1));
+  P->o_H = cv.take(8 * (size_t)B * kMaxRestart * (kMaxRestart + 1));
+  P->o_h1 = cv.take(8 * (size_t)B * (kMaxRestart + 1));
+  P->o_h2 = cv.take(8 * (size_t)B * (kMaxRestart + 1));
+  P->o_y = cv.take(8 * (size_t)B * kMaxRestart);
+  P->o_lsq = cv.take(8 * (size_t)B * 3 * (kMaxRestart + 1));
+  P->o_wn0 = cv.take(8 * (size_t)B);
+  P->o_circ = cv.take(8 * (size_t)B);
+  P->o_circ_rk = cv.take(8 * (size_t)B);
+  P->o_tpart = cv.take(8 * kTilePartStride * P->tiles.size());
+  P->pstride = P->m + 2;
+  P->o_cpart = cv.take(8 * (size_t)P->pstride * P->chunks.size());
+  P->o_cpartn = cv.take(8 * P->chunks.size());
+  P->o_coef = cv.take(8 * 3 * (size_t)B);
+  P->o_cp = cv.take(8 * (size_t)P->total_ni);
+  P->o_hrn = cv.take(8 * (size_t)B * P->p.max_iter);
+  P->o_hcl = cv.take(8 * (size_t)B * P->p.max_iter);
+  P->o_cnt = cv.take(8);
+  P->bytes = cv.off + 256;
+}
+
+// ---------------------------------------------------------------------------
+// kernels of this file: init, counting, layout conversion, point flux
+// ---------------------------------------------------------------------------
+__global__ void k_init_state(Batch b, double* U) {
+  const Tile t = b.tiles[blockIdx.x];
+  const CaseDev& cs = b.cases[t.cs];
+  const GridDev& g = cs.g;
+  const double rho = cs.winf[0], u = cs.winf[1], v = cs.winf[2], p = cs.winf[3];
+  const double Uc[4] = {rho, rho * u, rho * v, p / kGm1 + 0.5 * rho * (u * u + v * v)};
+  for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
+    const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) U[4 * cs.cell_off + vidx(g, k, j, i)] = Uc[k];
+  }
+}
+
+__global__ void k_reset(int ncases, CaseCtl* ctl, uint32_t* live, double cfl0) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ncases) return;
+  CaseCtl c{};
+  c.cfl = cfl0;
+  c.rn = NAN;
+  c.lastrn = NAN;
+  c.r0 = 1.0;
+  c.omega = 1.0;
+  ctl[k] = c;
+  live[k] = kLiveNewton;
+}
+
+__global__ void k_count(int ncases, const CaseCtl* ctl, const uint32_t* live, int retire, int* out) {
+  __shared__ int s;
+  if (threadIdx.x == 0) s = 0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < ncases; k += blockDim.x) {
+    const int busy = retire ? ((live[k] & kLiveNewton) ? 1 : 0) : (ctl[k].done ? 0 : 1);
+    if (busy) atomicAdd(&s, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *out = s;
+}
+
+// reference layout [4][ni][nc] <-> internal [4][nc][ni] of one case
+__global__ void k_to_internal(int ni, int nc, const double* __restrict__ src, double* __restrict__ dst) {
+  const size_t n = 4 * (size_t)ni * nc;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t / ((size_t)ni * nc));
+    const size_t r = t % ((size_t)ni * nc);
+    const int i = (int)(r / nc), j = (int)(r % nc);
+    dst[((size_t)k * nc + j) * ni + i] = src[t];
+  }
+}
+__global__ void k_to_reference(int ni, int nc, const double* __restrict__ src, double* __restrict__ dst) {
+  const size_t n = 4 * (size_t)ni * nc;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t / ((size_t)ni * nc));
+    const size_t r = t % ((size_t)ni * nc);
+    const int i = (int)(r / nc), j = (int)(r % nc);
+    dst[t] = src[((size_t)k * nc + j) * ni + i];
+  }
+}
+
+__global__ void k_point_flux(int n, const double* WL, const double* WR, const double* S, double* F) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  State4<double> L, R;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    L.c[k] = WL[(size_t)k * n + q];
+    R.c[k] = WR[(size_t)k * n + q];
+  }
+  const State4<double> f = hllc<double, double>(L, R, S[q], S[(size_t)n + q]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) F[(size_t)k * n + q] = f.c[k];
+}
+
+}  // namespace a2d
+
+// ---------------------------------------------------------------------------
+// orchestration
+// ---------------------------------------------------------------------------
+namespace a2d {
+
+template <typename TJ>
+static void precond(a2d_plan* P, const Batch& B, const double* rin, double* dst, uint32_t need, cudaStream_t s) {
+  SweepArgs a;
+  a.INV = P->at<double>(P->o_INV);
+  a.CF = P->at<double>(P->o_CF);
+  a.JJL = P->at<void>(P->o_JJL);
+  a.JIL = P->at<void>(P->o_JIL);
+  a.JIR = P->at<void>(P->o_JIR);
+  a.need = need;
+  a.r = rin;
+  const int sweeps = std::max(1, P->p.jacobi_sweeps);
+  double* bufs[2] = {P->vec(kPA), P->vec(kPB)};
+  const double* prev = nullptr;
+  for (int sw = 0; sw < sweeps; ++sw) {
+    double* out = (sw == sweeps - 1) ? dst : bufs[sw & 1];
+    a.xprev = prev;
+    a.out = out;
+    launch_sweep<TJ>(B, a, s);
+    prev = out;
+  }
+}
+
+template <typename TJ>
+static void precond_setup(a2d_plan* P, const Batch& B, uint32_t need, cudaStream_t s) {
+  JacArgs ja;
+  ja.U = P->vec(kU);
+  ja.circ = P->at<double>(P->o_circ);
+  ja.JIL = P->at<void>(P->o_JIL);
+  ja.JIR = P->at<void>(P->o_JIR);
+  ja.JJL = P->at<void>(P->o_JJL);
+  ja.JJR = P->at<void>(P->o_JJR);
+  ja.vortex = P->p.vortex_correction;
+  ja.need = need;
+  launch_face_jac<TJ>(B, ja, s);
+  FactorArgs fa;
+  fa.U = P->vec(kU);
+  fa.ctl = P->ctl();
+  fa.JIL = ja.JIL;
+  fa.JIR = ja.JIR;
+  fa.JJL = ja.JJL;
+  fa.JJR = ja.JJR;
+  fa.INV = P->at<double>(P->o_INV);
+  fa.CF = P->at<double>(P->o_CF);
+  fa.diag = P->at<double>(P->o_diag);
+  fa.cfl_base = P->p.cfl;
+  fa.need = need;
+  launch_factor<TJ>(B, fa, s);
+}
+
+static StencilArgs<double> residual_args(a2d_plan* P) {
+  StencilArgs<double> a;
+  a.U = P->vec(kU);
+  a.lim_k = P->p.lim_k;
+  a.order = P->p.order;
+  a.vortex = P->p.vortex_correction;
+  return a;
+}
+
+template <typename TV, typename TJ, typename TB>
+static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
+  const Batch& B = P->batch;
+  const uint32_t NW = kLiveNewton, KR = kLiveNewton | kLiveKrylov;
+  double* U = P->vec(kU);
+  double* b = P->vec(kB);
+  double* x0 = P->vec(kX0);
+  double* t = P->vec(kT);
+  double* r = P->vec(kRr);
+  double* z = P->vec(kZ);
+  double* w = P->vec(kW);
+  double* dU = P->vec(kDU);
+  double* diag = P->at<double>(P->o_diag);
+  double* tpart = P->at<double>(P->o_tpart);
+  double* cpart = P->at<double>(P->o_cpart);
+  double* cpartn = P->at<double>(P->o_cpartn);
+  TB* V = P->at<TB>(P->o_V);
+  const size_t vs = 4 * (size_t)P->C;
+  CaseCtl* ctl = P->ctl();
+  uint32_t* live = P->live();
+
+  launch_mark_stepped(B, live, ctl, s);
+  // Newton right-hand side b = -R(U) in FP64, circulation from U, residual-norm partials
+  StencilArgs<double> ra = residual_args(P);
+  ra.out = b;
+  ra.sign = -1.0;
+  ra.circ_out = P->at<double>(P->o_circ);
+  ra.tile_part = tpart;
+  ra.need = NW;
+  launch_stencil<double, false, double>(B, ra, s);
+  // line preconditioner at U
+  precond_setup<TJ>(P, B, NW, s);
+  // x0 = M b; ptol from ||b||, ||M b||
+  precond<TJ>(P, B, b, x0, NW, s);
+  launch_norms2(B, b, x0, cpart, P->pstride, NW, s);
+  launch_gm_setup(B, cpart, P->pstride, ctl, P->p.gmres_tol, s);
+  // t = b - A x0, A v = diag v + J v
+  StencilArgs<double> ta = residual_args(P);
+  ta.V = x0;
+  ta.diag = diag;
+  ta.bvec = b;
+  ta.out = t;
+  ta.need = NW;
+  launch_stencil<TV, true, double>(B, ta, s);
+  // r = M t, v0 = r / ||r||
+  precond<TJ>(P, B, t, r, NW, s);
+  launch_norm1(B, r, cpartn, NW, s);
+  NormalizeArgs<TB> n0;
+  n0.w = r;
+  n0.Vout = V;
+  n0.part_norm = cpartn;
+  n0.ctl = ctl;
+  n0.live = live;
+  n0.k = -1;
+  n0.need = NW;
+  launch_normalize<TB>(B, n0, s);
+  double* h1 = P->at<double>(P->o_h1);
+  double* h2 = P->at<double>(P->o_h2);
+  double* wn0 = P->at<double>(P->o_wn0);
+  for (int k = 0; k < P->m; ++k) {
+    StencilArgs<TB> za;
+    za.U = U;
+    za.V = V + (size_t)k * vs;
+    za.diag = diag;
+    za.out = z;
+    za.lim_k = P->p.lim_k;
+    za.order = P->p.order;
+    za.vortex = P->p.vortex_correction;
+    za.need = KR;
+    launch_stencil<TV, true, TB>(B, za, s);
+    precond<TJ>(P, B, z, w, KR, s);
+    // classical Gram-Schmidt, two passes
+    DotArgs<TB> d;
+    d.w = w;
+    d.V = V;
+    d.vstride = vs;
+    d.nq = k + 1;
+    d.with_norm = 1;
+    d.part = cpart;
+    d.pstride = P->pstride;
+    d.need = KR;
+    launch_dots<TB>(B, d, s);
+    UpdateArgs<TB> u;
+    u.w = w;
+    u.V = V;
+    u.vstride = vs;
+    u.nq = k + 1;
+    u.part = cpart;
+    u.pstride = P->pstride;
+    u.hstore = h1;
+    u.wn0 = wn0;
+    u.need = KR;
+    launch_update<TB>(B, u, s);
+    d.with_norm = 0;
+    launch_dots<TB>(B, d, s);
+    u.hstore = h2;
+    u.wn0 = nullptr;
+    u.part_norm = cpartn;
+    launch_update<TB>(B, u, s);
+    NormalizeArgs<TB> nk;
+    nk.w = w;
+    nk.Vout = V + (size_t)(k + 1) * vs;
+    nk.part_norm = cpartn;
+    nk.wn0 = wn0;
+    nk.h1 = h1;
+    nk.h2 = h2;
+    nk.H = P->at<double>(P->o_H);
+    nk.ctl = ctl;
+    nk.live = live;
+    nk.k = k;
+    nk.need = KR;
+    launch_normalize<TB>(B, nk, s);
+  }
+  launch_lstsq(B, live, ctl, P->at<double>(P->o_H), P->at<double>(P->o_y), P->at<double>(P->o_lsq), s);
+  CombineArgs<TB> ca;
+  ca.x0 = x0;
+  ca.V = V;
+  ca.vstride = vs;
+  ca.y = P->at<double>(P->o_y);
+  ca.ctl = ctl;
+  ca.out = dU;
+  ca.need = NW;
+  launch_combine<TB>(B, ca, s);
+  // positivity step limit, finiteness, per-case controller, commit, forces
+  launch_update_rel(B, U, dU, tpart, NW, s);
+  launch_update_check(B, U, dU, tpart, ctl, P->p.max_update, NW, s);
+  CtlParams cp;
+  cp.cfl0 = P->p.cfl0;
+  cp.cfl_max = P->p.cfl_max;
+  cp.tol = P->p.tol;
+  cp.retire = P->p.retire;
+  launch_controller(B, tpart, ctl, live, P->at<double>(P->o_hrn), P->p.max_iter, cp, s);
+  launch_commit(B, U, dU, ctl, s);
+  launch_forces(B, U, P->at<double>(P->o_coef), P->at<double>(P->o_cp), P->at<long long>(P->o_cpoff), ctl,
+                P->at<double>(P->o_hcl), P->p.max_iter, s);
+}
+
+static void newton_dispatch(a2d_plan* P, cudaStream_t s) {
+  if (P->p.precision == A2D_MIXED) newton_step_launches<float, float, float>(P, s);
+  else newton_step_launches<double, double, double>(P, s);
+}
+
+static int newton_step(a2d_plan* P, cudaStream_t s) {
+  if (!P->p.use_graph) {
+    newton_dispatch(P, s);
+    A2D_CK(cudaGetLastError());
+    return A2D_OK;
+  }
+  if (P->graph == nullptr) {
+    cudaStream_t cap;
+    A2D_CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    A2D_CK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    newton_dispatch(P, cap);
+    cudaError_t e = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (e != cudaSuccess) return fail(A2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&P->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(A2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  A2D_CK(cudaGraphLaunch(P->graph, s));
+  return A2D_OK;
+}
+
+}  // namespace a2d
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+#define A2D_BOUND(P)                                                     \
+  do {                                                                   \
+    if ((P) == nullptr) return fail(A2D_ERR_ARG, "null plan");           \
+    if ((P)->ws == nullptr) return fail(A2D_ERR_STATE, "plan not bound"); \
+  } while (0)
+
+extern "C" {
+
+int a2d_version(void) { return 100; }
+
+const char* a2d_last_error(void) { return g_last_error.c_str(); }
+
+void a2d_default_params(a2d_params* p) {
+  if (p == nullptr) return;
+  p->gmres_restart = 50;
+  p->jacobi_sweeps = 4;
+  p->gmres_tol = 0.01;
+  p->cfl0 = 10.0;
+  p->cfl_max = 300.0;
+  p->max_update = 0.2;
+  p->tol = 1e-8;
+  p->cfl = 2.5;
+  p->irs_eps = 0.6;
+  p->lim_k = 0.02;
+  p->order = 2;
+  p->vortex_correction = 1;
+  p->precision = A2D_FP64;
+  p->retire = 1;
+  p->max_iter = 200;
+  p->use_graph = 1;
+}
+
+int a2d_metrics_bytes(int ni, int nj, size_t* bytes) {
+  if (bytes == nullptr || ni < 4 || nj < 3) return fail(A2D_ERR_ARG, "metrics: need ni >= 4, nj >= 3");
+  *bytes = metrics_total_bytes(ni, nj - 1);
+  return A2D_OK;
+}
+
+int a2d_metrics_build(int ni, int nj, const double* x, const double* y, void* metrics, void* stream) {
+  if (x == nullptr || y == nullptr || metrics == nullptr || ni < 4 || nj < 3)
+    return fail(A2D_ERR_ARG, "metrics: bad arguments");
+  const int nc = nj - 1;
+  double* md = static_cast<double*>(metrics);
+  float* mf = reinterpret_cast<float*>(static_cast<char*>(metrics) +
+                                       ((metrics_doubles(ni, nc) * 8 + 255) & ~size_t(255)));
+  launch_metrics(ni, nc, x, y, md, mf, static_cast<cudaStream_t>(stream));
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_plan_create(int ncases, const int* ni, const int* nc, const void* const* metrics, const double* winf,
+                    const a2d_params* params, a2d_plan** out) {
+  if (out == nullptr || ncases <= 0 || ni == nullptr || nc == nullptr || metrics == nullptr || winf == nullptr)
+    return fail(A2D_ERR_ARG, "plan_create: bad arguments");
+  a2d_params p;
+  a2d_default_params(&p);
+  if (params != nullptr) p = *params;
+  if (p.gmres_restart < 1 || p.gmres_restart > kMaxRestart)
+    return fail(A2D_ERR_ARG, "gmres_restart must be in [1, 64]");
+  if (p.jacobi_sweeps < 1) return fail(A2D_ERR_ARG, "jacobi_sweeps must be >= 1");
+  if (p.order != 1 && p.order != 2) return fail(A2D_ERR_ARG, "order must be 1 or 2");
+  if (p.precision != A2D_FP64 && p.precision != A2D_MIXED) return fail(A2D_ERR_ARG, "unknown precision");
+  if (p.max_iter < 1) return fail(A2D_ERR_ARG, "max_iter must be >= 1");
+  for (int k = 0; k < ncases; ++k) {
+    if (ni[k] < 4 || nc[k] < 2 || metrics[k] == nullptr)
+      return fail(A2D_ERR_ARG, "case " + std::to_string(k) + ": need ni >= 4, nc >= 2 and metrics");
+  }
+  a2d_plan* P = new a2d_plan();
+  P->p = p;
+  P->ncases = ncases;
+  P->m = p.gmres_restart;
+  P->tj = p.precision == A2D_MIXED ? 4 : 8;
+  P->tb = p.precision == A2D_MIXED ? 4 : 8;
+  build_tables(P, ni, nc, metrics, winf);
+  layout(P);
+  *out = P;
+  return A2D_OK;
+}
+
+int a2d_plan_workspace_bytes(const a2d_plan* P, size_t* bytes) {
+  if (P == nullptr || bytes == nullptr) return fail(A2D_ERR_ARG, "null argument");
+  *bytes = P->bytes;
+  return A2D_OK;
+}
+
+int a2d_plan_ncases(const a2d_plan* P) { return P ? P->ncases : 0; }
+
+int a2d_plan_bind(a2d_plan* P, void* workspace, size_t bytes, void* stream) {
+  if (P == nullptr || workspace == nullptr) return fail(A2D_ERR_ARG, "bind: null argument");
+  if (bytes < P->bytes) return fail(A2D_ERR_ARG, "bind: workspace too small");
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return fail(A2D_ERR_ARG, "bind: workspace not 256-byte aligned");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (P->graph != nullptr) {
+    cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+  }
+  P->ws = static_cast<char*>(workspace);
+  A2D_CK(cudaMemcpyAsync(P->ws + P->o_cases, P->cases.data(), sizeof(CaseDev) * P->ncases,
+                         cudaMemcpyHostToDevice, s));
+  A2D_CK(cudaMemcpyAsync(P->ws + P->o_tiles, P->tiles.data(), sizeof(Tile) * P->tiles.size(),
+                         cudaMemcpyHostToDevice, s));
+  A2D_CK(cudaMemcpyAsync(P->ws + P->o_chunks, P->chunks.data(), sizeof(Chunk) * P->chunks.size(),
+                         cudaMemcpyHostToDevice, s));
+  A2D_CK(cudaMemcpyAsync(P->ws + P->o_groups, P->groups.data(), sizeof(Group) * P->groups.size(),
+                         cudaMemcpyHostToDevice, s));
+  A2D_CK(cudaMemcpyAsync(P->ws + P->o_cpoff, P->cp_off.data(), sizeof(long long) * P->ncases,
+                         cudaMemcpyHostToDevice, s));
+  A2D_CK(cudaMemsetAsync(P->ws + P->o_vec[0], 0, P->o_diag - P->o_vec[0], s));
+  Batch& B = P->batch;
+  B.cases = P->at<CaseDev>(P->o_cases);
+  B.tiles = P->at<Tile>(P->o_tiles);
+  B.chunks = P->at<Chunk>(P->o_chunks);
+  B.groups = P->at<Group>(P->o_groups);
+  B.live = P->live();
+  B.ncases = P->ncases;
+  B.ntiles = (int)P->tiles.size();
+  B.nchunks = (int)P->chunks.size();
+  B.ngroups = (int)P->groups.size();
+  if (P->host_count == nullptr) A2D_CK(cudaMallocHost(&P->host_count, sizeof(int)));
+  k_reset<<<(P->ncases + 63) / 64, 64, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.cfl0);
+  A2D_CK(cudaMemsetAsync(P->ws + P->o_circ_rk, 0, 8 * (size_t)P->ncases, s));
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_plan_destroy(a2d_plan* P) {
+  if (P == nullptr) return A2D_OK;
+  if (P->graph != nullptr) cudaGraphExecDestroy(P->graph);
+  if (P->host_count != nullptr) cudaFreeHost(P->host_count);
+  delete P;
+  return A2D_OK;
+}
+
+static int check_case(const a2d_plan* P, int slot, int k) {
+  if (slot < 0 || slot > A2D_VEC_DU) return fail(A2D_ERR_ARG, "unknown vector slot");
+  if (k < 0 || k >= P->ncases) return fail(A2D_ERR_ARG, "case index out of range");
+  return A2D_OK;
+}
+
+int a2d_vec_set(a2d_plan* P, int slot, int k, const double* src, void* stream) {
+  A2D_BOUND(P);
+  if (int e = check_case(P, slot, k)) return e;
+  if (src == nullptr) return fail(A2D_ERR_ARG, "null source");
+  const CaseDev& c = P->cases[k];
+  k_to_internal<<<256, 256, 0, static_cast<cudaStream_t>(stream)>>>(c.g.ni, c.g.nc, src,
+                                                                     P->vec(slot) + 4 * c.cell_off);
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_vec_get(const a2d_plan* P, int slot, int k, double* dst, void* stream) {
+  A2D_BOUND(P);
+  if (int e = check_case(P, slot, k)) return e;
+  if (dst == nullptr) return fail(A2D_ERR_ARG, "null destination");
+  const CaseDev& c = P->cases[k];
+  k_to_reference<<<256, 256, 0, static_cast<cudaStream_t>(stream)>>>(c.g.ni, c.g.nc,
+                                                                      P->vec(slot) + 4 * c.cell_off, dst);
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_init_freestream(a2d_plan* P, void* stream) {
+  A2D_BOUND(P);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_init_state<<<P->batch.ntiles, 256, 0, s>>>(P->batch, P->vec(kU));
+  k_reset<<<(P->ncases + 63) / 64, 64, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.cfl0);
+  A2D_CK(cudaGetLastError());
+  P->steps_taken = 0;
+  return A2D_OK;
+}
+
+int a2d_reset(a2d_plan* P, void* stream) {
+  A2D_BOUND(P);
+  k_reset<<<(P->ncases + 63) / 64, 64, 0, static_cast<cudaStream_t>(stream)>>>(P->ncases, P->ctl(), P->live(),
+                                                                                P->p.cfl0);
+  A2D_CK(cudaGetLastError());
+  P->steps_taken = 0;
+  return A2D_OK;
+}
+
+int a2d_residual(a2d_plan* P, const double* circ, void* stream) {
+  A2D_BOUND(P);
+  StencilArgs<double> a = residual_args(P);
+  a.circ_in = circ;
+  a.out = P->vec(kR);
+  a.sign = 1.0;
+  a.circ_out = P->at<double>(P->o_circ);
+  a.tile_part = P->at<double>(P->o_tpart);
+  Batch B = P->batch;
+  B.live = nullptr;
+  launch_stencil<double, false, double>(B, a, static_cast<cudaStream_t>(stream));
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_jvp(a2d_plan* P, void* stream) {
+  A2D_BOUND(P);
+  StencilArgs<double> a = residual_args(P);
+  a.V = P->vec(kVin);
+  a.out = P->vec(kJV);
+  Batch B = P->batch;
+  B.live = nullptr;
+  if (P->p.precision == A2D_MIXED) launch_stencil<float, true, double>(B, a, static_cast<cudaStream_t>(stream));
+  else launch_stencil<double, true, double>(B, a, static_cast<cudaStream_t>(stream));
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_forces(a2d_plan* P, double* coef, double* cp, void* stream) {
+  A2D_BOUND(P);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Batch B = P->batch;
+  B.live = nullptr;
+  launch_forces(B, P->vec(kU), P->at<double>(P->o_coef), P->at<double>(P->o_cp), P->at<long long>(P->o_cpoff),
+                nullptr, nullptr, 0, s);
+  if (coef != nullptr)
+    A2D_CK(cudaMemcpyAsync(coef, P->at<double>(P->o_coef), 8 * 3 * (size_t)P->ncases, cudaMemcpyDeviceToDevice, s));
+  if (cp != nullptr)
+    A2D_CK(cudaMemcpyAsync(cp, P->at<double>(P->o_cp), 8 * (size_t)P->total_ni, cudaMemcpyDeviceToDevice, s));
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_set_cfl(a2d_plan* P, const double* cfl, void* stream) {
+  A2D_BOUND(P);
+  if (cfl == nullptr) return fail(A2D_ERR_ARG, "null cfl");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (int k = 0; k < P->ncases; ++k)
+    A2D_CK(cudaMemcpyAsync(&P->ctl()[k].cfl, &cfl[k], sizeof(double), cudaMemcpyHostToDevice, s));
+  A2D_CK(cudaStreamSynchronize(s));
+  return A2D_OK;
+}
+
+int a2d_precond_setup(a2d_plan* P, void* stream) {
+  A2D_BOUND(P);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // circulation of U for the far-field block (as the Newton step forms it)
+  StencilArgs<double> a = residual_args(P);
+  a.out = P->vec(kB);
+  a.sign = -1.0;
+  a.circ_out = P->at<double>(P->o_circ);
+  a.tile_part = P->at<double>(P->o_tpart);
+  Batch B = P->batch;
+  B.live = nullptr;
+  launch_stencil<double, false, double>(B, a, s);
+  if (P->p.precision == A2D_MIXED) precond_setup<float>(P, B, 0, s);
+  else precond_setup<double>(P, B, 0, s);
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_precond_apply(a2d_plan* P, void* stream) {
+  A2D_BOUND(P);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Batch B = P->batch;
+  B.live = nullptr;
+  if (P->p.precision == A2D_MIXED) precond<float>(P, B, P->vec(kVin), P->vec(kJV), 0, s);
+  else precond<double>(P, B, P->vec(kVin), P->vec(kJV), 0, s);
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_newton_step(a2d_plan* P, void* stream) {
+  A2D_BOUND(P);
+  const int e = newton_step(P, static_cast<cudaStream_t>(stream));
+  if (e == A2D_OK) P->steps_taken += 1;
+  return e;
+}
+
+int a2d_newton_run(a2d_plan* P, int max_steps, int* steps, void* stream) {
+  A2D_BOUND(P);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int done = 0;
+  int* dcount = P->at<int>(P->o_cnt);
+  for (int it = 0; it < max_steps; ++it) {
+    if (P->steps_taken >= P->p.max_iter) break;
+    if (int e = newton_step(P, s)) return e;
+    P->steps_taken += 1;
+    ++done;
+    k_count<<<1, 256, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.retire, dcount);
+    A2D_CK(cudaMemcpyAsync(P->host_count, dcount, sizeof(int), cudaMemcpyDeviceToHost, s));
+    A2D_CK(cudaStreamSynchronize(s));
+    if (*P->host_count == 0) break;
+  }
+  if (steps != nullptr) *steps = done;
+  return A2D_OK;
+}
+
+int a2d_case_status(const a2d_plan* P, int* nsteps, int* done, int* frozen, double* lastrn, double* r0,
+                    void* stream) {
+  A2D_BOUND(P);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  std::vector<CaseCtl> h(P->ncases);
+  A2D_CK(cudaMemcpyAsync(h.data(), P->ctl(), sizeof(CaseCtl) * P->ncases, cudaMemcpyDeviceToHost, s));
+  A2D_CK(cudaStreamSynchronize(s));
+  for (int k = 0; k < P->ncases; ++k) {
+    if (nsteps) nsteps[k] = h[k].nsteps;
+    if (done) done[k] = h[k].done;
+    if (frozen) frozen[k] = h[k].frozen;
+    if (lastrn) lastrn[k] = h[k].lastrn;
+    if (r0) r0[k] = h[k].r0;
+  }
+  return A2D_OK;
+}
+
+int a2d_case_scalars(const a2d_plan* P, double* out, void* stream) {
+  A2D_BOUND(P);
+  if (out == nullptr) return fail(A2D_ERR_ARG, "null output");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  std::vector<CaseCtl> h(P->ncases);
+  std::vector<double> circ(P->ncases);
+  A2D_CK(cudaMemcpyAsync(h.data(), P->ctl(), sizeof(CaseCtl) * P->ncases, cudaMemcpyDeviceToHost, s));
+  A2D_CK(cudaMemcpyAsync(circ.data(), P->at<double>(P->o_circ), 8 * (size_t)P->ncases, cudaMemcpyDeviceToHost, s));
+  A2D_CK(cudaStreamSynchronize(s));
+  for (int k = 0; k < P->ncases; ++k) {
+    double* o = out + 8 * (size_t)k;
+    o[0] = h[k].rn;
+    o[1] = h[k].omega;
+    o[2] = h[k].cfl;
+    o[3] = h[k].r0;
+    o[4] = circ[k];
+    o[5] = h[k].beta;
+    o[6] = (double)h[k].k_used;
+    o[7] = (double)h[k].commit;
+  }
+  return A2D_OK;
+}
+
+int a2d_history(const a2d_plan* P, int steps, double* rn, double* cl, void* stream) {
+  A2D_BOUND(P);
+  if (steps < 0 || steps > P->p.max_iter) return fail(A2D_ERR_ARG, "history: steps out of range");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t n = (size_t)steps * P->ncases * 8;
+  if (rn != nullptr && n) A2D_CK(cudaMemcpyAsync(rn, P->at<double>(P->o_hrn), n, cudaMemcpyDeviceToHost, s));
+  if (cl != nullptr && n) A2D_CK(cudaMemcpyAsync(cl, P->at<double>(P->o_hcl), n, cudaMemcpyDeviceToHost, s));
+  A2D_CK(cudaStreamSynchronize(s));
+  return A2D_OK;
+}
+
+int a2d_set_circulation(a2d_plan* P, const double* circ, void* stream) {
+  A2D_BOUND(P);
+  if (circ == nullptr) return fail(A2D_ERR_ARG, "null circulation");
+  A2D_CK(cudaMemcpyAsync(P->at<double>(P->o_circ_rk), circ, 8 * (size_t)P->ncases, cudaMemcpyHostToDevice,
+                         static_cast<cudaStream_t>(stream)));
+  return A2D_OK;
+}
+
+int a2d_smooth(a2d_plan* P, void* stream) {
+  A2D_BOUND(P);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Batch B = P->batch;
+  B.live = nullptr;
+  launch_irs(B, P->vec(kR), P->vec(kPA), P->p.irs_eps, P->max_ni, P->max_nc, s);
+  if (P->p.irs_eps > 0)
+    A2D_CK(cudaMemcpyAsync(P->vec(kR), P->vec(kPA), 8 * 4 * (size_t)P->C, cudaMemcpyDeviceToDevice, s));
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_rk_iterate(a2d_plan* P, int n, double* res, void* stream) {
+  A2D_BOUND(P);
+  if (n < 0) return fail(A2D_ERR_ARG, "negative iteration count");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Batch B = P->batch;
+  B.live = nullptr;
+  double* U = P->vec(kU);
+  double* U0 = P->vec(kU0);
+  double* R = P->vec(kR);
+  double* Rs = P->vec(kPA);
+  double* dt = P->at<double>(P->o_dt);
+  double* circ = P->at<double>(P->o_circ_rk);
+  double* tpart = P->at<double>(P->o_tpart);
+  const double alphas[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
+  for (int it = 0; it < n; ++it) {
+    A2D_CK(cudaMemcpyAsync(U0, U, 8 * 4 * (size_t)P->C, cudaMemcpyDeviceToDevice, s));
+    launch_local_dt(B, U, dt, P->p.cfl, s);
+    for (int st = 0; st < 4; ++st) {
+      StencilArgs<double> a = residual_args(P);
+      a.circ_in = circ;
+      a.out = R;
+      a.sign = 1.0;
+      launch_stencil<double, false, double>(B, a, s);
+      const double* Ruse = R;
+      if (P->p.irs_eps > 0) {
+        launch_irs(B, R, Rs, P->p.irs_eps, P->max_ni, P->max_nc, s);
+        Ruse = Rs;
+      }
+      launch_rk_stage(B, U0, Ruse, dt, U, alphas[st], s);
+    }
+    launch_rk_res(B, U0, U, dt, tpart, s);
+    launch_forces(B, U, P->at<double>(P->o_coef), P->at<double>(P->o_cp), P->at<long long>(P->o_cpoff), nullptr,
+                  nullptr, 0, s);
+    launch_rk_finish(B, tpart, P->at<double>(P->o_coef), (it == n - 1) ? res : nullptr, circ, s);
+  }
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_hllc_flux(int n, const double* WL, const double* WR, const double* S, double* F, void* stream) {
+  if (n < 0 || (n > 0 && (WL == nullptr || WR == nullptr || S == nullptr || F == nullptr)))
+    return fail(A2D_ERR_ARG, "hllc_flux: bad arguments");
+  if (n == 0) return A2D_OK;
+  k_point_flux<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(n, WL, WR, S, F);
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+/*
+ * aero2d_b200 — C ABI of the batched 2-D Euler solver path of aero2d, for B200 (sm_100a).
+ *
+ * The reference (Bulbulator72/Aero2d) is Python + JAX and binds no native
+ * code; each entry point below replaces one JAX computation of its Euler path
+ * and is called through ctypes from the Python classes aero2d_b200.euler and
+ * aero2d_b200.implicit, which keep the reference's class names, arguments and
+ * error behaviour.  Conventions:
+ *   - every function returns an int status (A2D_OK = 0); no C++ exception
+ *     crosses the ABI; a2d_last_error() describes the last failure of the
+ *     calling thread;
+ *   - the caller owns all device memory: it allocates the grid-metrics blob
+ *     and the plan workspace (sizes from the *_bytes queries) and passes
+ *     plain device pointers; the library allocates no device memory;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream);
+ *   - arrays handed in and out use the reference's layouts: node coordinates
+ *     x[i][j] (ni x nj, i along the contour, j from the wall outward), states
+ *     U[4][ni][nc] per case (conserved rho, rho u, rho v, E), per-case freestream
+ *     primitives winf[4] = (rho, u, v, p).
+ * A plan is used by one host thread at a time (one plan per GUI worker or
+ * request loop); distinct plans are independent.
+ */
+#ifndef AERO2D_B200_H
+#define AERO2D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define A2D_OK 0
+#define A2D_ERR_ARG 1      /* invalid argument (sizes, null pointers, unbound plan) */
+#define A2D_ERR_CUDA 2     /* a CUDA call failed */
+#define A2D_ERR_STATE 3    /* call out of order (plan not bound, no step taken) */
+
+#define A2D_FP64 0         /* every stage in FP64 */
+#define A2D_MIXED 1        /* JVP, face Jacobians and Krylov basis in FP32; residual,
+                              factorisation, Gram-Schmidt, norms, update in FP64 */
+
+/* vector slots of a bound plan (packed over the cases of the plan) */
+#define A2D_VEC_U 0        /* conserved state */
+#define A2D_VEC_R 1        /* residual output of a2d_residual */
+#define A2D_VEC_V 2        /* direction input of a2d_jvp / a2d_precond_apply */
+#define A2D_VEC_JV 3       /* output of a2d_jvp / a2d_precond_apply */
+#define A2D_VEC_DU 4       /* Newton update of the last step */
+
+typedef struct a2d_plan a2d_plan;
+
+/* Solver settings; names follow EulerSolver (aero2d/euler.py:219-221) and
+ * ImplicitEuler (aero2d/implicit.py:68-70) and their solve() arguments. */
+typedef struct a2d_params {
+  int gmres_restart;      /* ImplicitEuler gmres_restart (<= 64)            default 50   */
+  int jacobi_sweeps;      /* ImplicitEuler jacobi_sweeps                    default 4    */
+  double gmres_tol;       /* ImplicitEuler gmres_tol                        default 0.01 */
+  double cfl0;            /* ImplicitEuler cfl0                             default 10   */
+  double cfl_max;         /* ImplicitEuler cfl_max                          default 300  */
+  double max_update;      /* ImplicitEuler max_update                       default 0.2  */
+  double tol;             /* ImplicitEuler.solve tol (residual drop)        default 1e-8 */
+  double cfl;             /* EulerSolver cfl (explicit CFL, local_dt)       default 2.5  */
+  double irs_eps;         /* EulerSolver irs_eps                            default 0.6  */
+  double lim_k;           /* EulerSolver lim_k                              default 0.02 */
+  int order;              /* EulerSolver order (1 or 2)                     default 2    */
+  int vortex_correction;  /* EulerSolver vortex_correction                  default 1    */
+  int precision;          /* A2D_FP64 or A2D_MIXED                          default FP64 */
+  int retire;             /* 1: a case stops stepping once done; 0: all cases step
+                             until every case is done (the reference loop) default 1    */
+  int max_iter;           /* capacity of the per-step history               default 200  */
+  int use_graph;          /* replay each Newton step as one CUDA graph      default 1    */
+} a2d_params;
+
+int a2d_version(void);
+const char* a2d_last_error(void);
+void a2d_default_params(a2d_params* params);
+
+/* ---- grid metrics (aero2d/euler.py:44-60 compute_metrics, :230-233 xf/yf) ---- */
+int a2d_metrics_bytes(int ni, int nj, size_t* bytes);
+/* x, y: device FP64 node coordinates [ni][nj]; metrics: device blob of a2d_metrics_bytes */
+int a2d_metrics_build(int ni, int nj, const double* x, const double* y, void* metrics, void* stream);
+
+/* ---- plans: a batch of cases (the vmap axis of euler.py:393 / implicit.py:204-210) ---- */
+/* ni[k], nc[k]: cells of case k; metrics[k]: its metrics blob; winf: [ncases][4] host FP64 */
+int a2d_plan_create(int ncases, const int* ni, const int* nc, const void* const* metrics,
+                    const double* winf, const a2d_params* params, a2d_plan** plan);
+int a2d_plan_workspace_bytes(const a2d_plan* plan, size_t* bytes);
+int a2d_plan_bind(a2d_plan* plan, void* workspace, size_t bytes, void* stream);
+int a2d_plan_destroy(a2d_plan* plan);
+int a2d_plan_ncases(const a2d_plan* plan);
+
+/* vector I/O in the reference layout [4][ni][nc] of one case (device pointers) */
+int a2d_vec_set(a2d_plan* plan, int slot, int case_index, const double* src, void* stream);
+int a2d_vec_get(const a2d_plan* plan, int slot, int case_index, double* dst, void* stream);
+
+/* ---- point operations (aero2d/euler.py) ---- */
+/* U of every case := prim_to_cons(winf) (init_state, euler.py:383-384); resets the Newton state */
+int a2d_init_freestream(a2d_plan* plan, void* stream);
+/* resets the Newton state (CFL, histories, flags) and keeps U (warm start U0) */
+int a2d_reset(a2d_plan* plan, void* stream);
+/* R := residual(U, winf, circ) (euler.py:259-287); circ: device [ncases] or NULL for
+ * Gamma(U) = Cl(U) M / 2 as ImplicitEuler._res does (implicit.py:160-167) */
+int a2d_residual(a2d_plan* plan, const double* circ, void* stream);
+/* JV := d residual(U, winf, Gamma(U)) / dU . V  (implicit.py:179-181, jax.jvp) */
+int a2d_jvp(a2d_plan* plan, void* stream);
+/* forces (euler.py:318-331): coef [ncases][3] = Cl, Cd, Cm; cp: wall Cp of all cases
+ * concatenated (ni per case), may be NULL; device pointers */
+int a2d_forces(a2d_plan* plan, double* coef, double* cp, void* stream);
+/* builds the line preconditioner at U with the per-case CFL (implicit.py:81-128) */
+int a2d_precond_setup(a2d_plan* plan, void* stream);
+/* JV := M(V), the line-Jacobi application (implicit.py:150-157) */
+int a2d_precond_apply(a2d_plan* plan, void* stream);
+/* sets the pseudo-time CFL of every case (host array [ncases]) */
+int a2d_set_cfl(a2d_plan* plan, const double* cfl, void* stream);
+
+/* ---- the Newton-Krylov solver (aero2d/implicit.py:169-253) ---- */
+/* one pseudo-transient Newton step of every live case, with the per-case
+ * rollback / freeze / SER-CFL logic of ImplicitEuler.solve on the device */
+int a2d_newton_step(a2d_plan* plan, void* stream);
+/* up to max_steps steps; stops when no case is live (retire=1) or every case is
+ * done (retire=0); *steps receives the number of steps taken; synchronises */
+int a2d_newton_run(a2d_plan* plan, int max_steps, int* steps, void* stream);
+/* per-case results to host arrays (any may be NULL), length ncases:
+ * nsteps, converged-to-tol flag, frozen flag, last finite residual norm, r0 */
+int a2d_case_status(const a2d_plan* plan, int* nsteps, int* done, int* frozen, double* lastrn,
+                    double* r0, void* stream);
+/* per-case scalars of the last step to a host array [ncases][8]: residual norm (NaN if the
+ * step failed), step length omega, CFL of the next step, r0, circulation, ||M(b - A x0)||,
+ * Arnoldi vectors used, 1 if the step was committed */
+int a2d_case_scalars(const a2d_plan* plan, double* out, void* stream);
+/* per-step histories to host arrays [steps][ncases] (residual norm, Cl); steps <= max_iter */
+int a2d_history(const a2d_plan* plan, int steps, double* rn, double* cl, void* stream);
+
+/* ---- explicit RK4 + implicit residual smoothing (aero2d/euler.py:334-346) ---- */
+/* n RK iterations of every case, each followed by circ := Cl M / 2 (euler.py:398-404);
+ * res: device [ncases], the RK residual of the last iteration */
+int a2d_rk_iterate(a2d_plan* plan, int n, double* res, void* stream);
+/* R := smooth(R) in place on the residual slot (euler.py:298-312) */
+int a2d_smooth(a2d_plan* plan, void* stream);
+/* per-case circulation slot used by a2d_rk_iterate: host array [ncases] */
+int a2d_set_circulation(a2d_plan* plan, const double* circ, void* stream);
+
+/* point-wise HLLC flux of n faces (euler.py:79-121): WL, WR [4][n], S [2][n], F [4][n]
+ * device FP64 arrays */
+int a2d_hllc_flux(int n, const double* WL, const double* WR, const double* S, double* F, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AERO2D_B200_H */

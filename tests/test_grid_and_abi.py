@@ -1,0 +1,90 @@
+"""Host-side checks without a GPU: the grid generator against the reference's
+grids, and the C ABI library (loads, exports every declared symbol, plans are
+laid out on the host)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from aero2d_b200 import _lib
+from aero2d_b200.geometry import naca4, naca4_params
+from aero2d_b200.grid import GridError, ogrid
+from tests.conftest import ROOT
+from tests.golden.make_golden import GRIDS
+
+
+@pytest.mark.parametrize("key", list(GRIDS))
+def test_grid_bit_identical_to_reference(ref_grids, key):
+    code, ns, nj, ds0, rad = GRIDS[key]
+    g = ogrid(naca4(code, ns), nj=nj, ds0=ds0, radius=rad)
+    assert np.array_equal(g.x, ref_grids[f"{key}_x"])
+    assert np.array_equal(g.y, ref_grids[f"{key}_y"])
+
+
+def test_float_naca_params_match_code():
+    a = naca4("2412", 65)
+    b = naca4_params(0.02, 0.4, 0.12, 65)
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+
+
+def test_inverted_grid_raises():
+    with pytest.raises(GridError):
+        ogrid(naca4("6412", 193), nj=97, ds0=1e-3, radius=20.0)
+
+
+def _declared_symbols():
+    hdr = (ROOT / "include" / "aero2d_b200.h").read_text()
+    return sorted(set(re.findall(r"\b(a2d_[a-z0-9_]+)\s*\(", hdr)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = _declared_symbols()
+    assert len(names) > 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+
+
+def test_params_struct_matches_header():
+    hdr = (ROOT / "include" / "aero2d_b200.h").read_text()
+    body = hdr[hdr.index("typedef struct a2d_params"):hdr.index("} a2d_params;")]
+    fields = re.findall(r"^\s*(?:int|double)\s+(\w+);", body, re.M)
+    assert fields == [f for f, _ in _lib.Params._fields_]
+
+
+def test_plan_layout_on_host():
+    """Plans are created and sized on the host; no device call is made."""
+    lib = _lib.load()
+    n = C.c_size_t()
+    _lib.check(lib.a2d_metrics_bytes(256, 65, C.byref(n)))
+    assert n.value > 0
+    B = 3
+    ni = (C.c_int * B)(256, 192, 128)
+    nc = (C.c_int * B)(64, 48, 32)
+    fake = (C.c_void_p * B)(4096, 8192, 16384)     # never dereferenced before bind
+    winf = (C.c_double * (4 * B))(*([1.0, 0.5, 0.0, 1 / 1.4] * B))
+    p = _lib.default_params()
+    h = C.c_void_p()
+    _lib.check(lib.a2d_plan_create(B, ni, nc, fake, winf, C.byref(p), C.byref(h)))
+    _lib.check(lib.a2d_plan_workspace_bytes(h, C.byref(n)))
+    cells = 256 * 64 + 192 * 48 + 128 * 32
+    assert n.value > 8 * 4 * cells * (p.gmres_restart + 1)
+    assert lib.a2d_plan_ncases(h) == B
+    assert lib.a2d_residual(h, None, None) == _lib.A2D_ERR_STATE     # unbound plan
+    _lib.check(lib.a2d_plan_destroy(h))
+
+
+def test_plan_rejects_bad_params():
+    lib = _lib.load()
+    p = _lib.default_params()
+    p.gmres_restart = 100
+    h = C.c_void_p()
+    ni = (C.c_int * 1)(64)
+    nc = (C.c_int * 1)(24)
+    m = (C.c_void_p * 1)(4096)
+    w = (C.c_double * 4)(1.0, 0.5, 0.0, 1 / 1.4)
+    assert lib.a2d_plan_create(1, ni, nc, m, w, C.byref(p), C.byref(h)) == _lib.A2D_ERR_ARG
+    assert b"gmres_restart" in lib.a2d_last_error()
