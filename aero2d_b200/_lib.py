@@ -22,6 +22,9 @@ A2D_MIXED = 1
 
 VEC_U, VEC_R, VEC_V, VEC_JV, VEC_DU = 0, 1, 2, 3, 4
 
+# kernels that a2d_time_kernel can time
+K_JVP, K_LINES, K_RHS, K_DOTS, K_UPDATE, K_RESIDUAL, K_FACEJAC, K_FACTOR = range(8)
+
 
 class ExtensionMissing(RuntimeError):
     """The CUDA library libaero2d_b200.so is not built or cannot be loaded."""
@@ -91,6 +94,9 @@ SIGNATURES = {
                              C.POINTER(_D), _P]),
     "a2d_case_scalars": (_I, [_P, C.POINTER(_D), _P]),
     "a2d_history": (_I, [_P, _I, C.POINTER(_D), C.POINTER(_D), _P]),
+    "a2d_live_count": (_I, [_P, C.POINTER(_I), _P]),
+    "a2d_plan_stats": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_SZ)]),
+    "a2d_time_kernel": (_I, [_P, _I, _I, C.POINTER(C.c_float), _P]),
     "a2d_rk_iterate": (_I, [_P, _I, _P, _P]),
     "a2d_smooth": (_I, [_P, _P]),
     "a2d_set_circulation": (_I, [_P, C.POINTER(_D), _P]),

@@ -42,22 +42,28 @@ struct FactorArgs {
   const void* JIR = nullptr;
   const void* JJL = nullptr;
   const void* JJR = nullptr;
-  double* INV = nullptr;           // inverse of the block-Thomas pivots [rows nc]
-  double* CF = nullptr;            // upper factors c_j                 [rows nc]
+  void* INV = nullptr;             // inverse of the block-Thomas pivots [rows nc]
+  void* CF = nullptr;              // upper factors c_j                 [rows nc]
+  void* G = nullptr;               // -inv_j A_j                         [rows nc]
   double* diag = nullptr;          // per-cell vol / dtau
   double cfl_base = 2.5;           // EulerSolver.cfl, which local_dt multiplies and step() divides out
   uint32_t need = 0;
 };
 
-struct SweepArgs {
-  const double* r = nullptr;       // right-hand side
+struct RhsArgs {
+  const double* r = nullptr;       // right-hand side of the preconditioner
   const double* xprev = nullptr;   // previous sweep (nullptr on the first sweep)
-  double* out = nullptr;
-  const double* INV = nullptr;
-  const double* CF = nullptr;
-  const void* JJL = nullptr;
+  double* out = nullptr;           // e = inv (r - off)
+  const void* INV = nullptr;
   const void* JIL = nullptr;
   const void* JIR = nullptr;
+  uint32_t need = 0;
+};
+
+struct LinesArgs {
+  double* x = nullptr;             // in: e, out: the line solution (in place)
+  const void* G = nullptr;
+  const void* CF = nullptr;
   uint32_t need = 0;
 };
 
@@ -73,10 +79,13 @@ void launch_forces(const Batch& b, const double* U, double* coef, double* cp, co
 template <typename T>
 void launch_face_jac(const Batch& b, const JacArgs& a, cudaStream_t s);
 
-template <typename TJ>
+template <typename TJ, typename TF>
 void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s);
 
-template <typename TJ>
-void launch_sweep(const Batch& b, const SweepArgs& a, cudaStream_t s);
+template <typename TJ, typename TF>
+void launch_rhs(const Batch& b, const RhsArgs& a, cudaStream_t s);
+
+template <typename TF>
+void launch_lines(const Batch& b, const LinesArgs& a, cudaStream_t s);
 
 }  // namespace a2d

@@ -7,11 +7,19 @@
 //  k_factor     assembles D = sum of face blocks + vol/dtau I and runs the
 //               block-Thomas forward elimination along each wall-normal line
 //               in FP64: den_j = D_j - A_j c_{j-1}, inv_j = den_j^-1,
-//               c_j = inv_j C_j (aero2d/implicit.py:81-128).  One thread per
-//               line, 32 lines (one warp) per line group.
-//  k_sweep      one line-Jacobi sweep: moves the i-coupling of the previous
-//               sweep to the right-hand side and solves every j-line with the
-//               stored factors (aero2d/implicit.py:130-157).
+//               c_j = inv_j C_j (aero2d/implicit.py:81-128), and stores inv_j,
+//               c_j and G_j = -inv_j A_j.  One thread per line, 32 lines (one
+//               warp) per line group.
+//  k_rhs        first half of a line-Jacobi sweep (aero2d/implicit.py:150-157):
+//               moves the i-coupling of the previous sweep to the right-hand
+//               side and applies inv_j, e_j = inv_j (r_j - off_j); fully
+//               parallel over cells.
+//  k_lines      second half: the sequential recurrences d_j = e_j + G_j d_{j-1}
+//               and x_j = d_j - c_j x_{j+1} along each line
+//               (aero2d/implicit.py:130-148), which equal the reference's
+//               d_j = inv_j (r_j - A_j d_{j-1}) in exact arithmetic.  Only 20
+//               words per step remain on the sequential path, loaded 4 steps
+//               ahead.
 //
 // The blocks are stored lane-blocked ([group][row][entry][lane]) so that at
 // every step of the sequential j recurrence a warp reads each matrix entry of
@@ -198,7 +206,7 @@ __device__ __forceinline__ void load_block(const TJ* base, long long row0, int r
   for (int e = 0; e < 16; ++e) A[e] = (double)base[lbidx(row0, rows, g, j, e, lane)];
 }
 
-template <typename TJ>
+template <typename TJ, typename TF>
 __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gid = blockIdx.x * 4 + warp;
@@ -216,6 +224,9 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   const TJ* JIR = static_cast<const TJ*>(a.JIR);
   const TJ* JJL = static_cast<const TJ*>(a.JJL);
   const TJ* JJR = static_cast<const TJ*>(a.JJR);
+  TF* INV = static_cast<TF*>(a.INV);
+  TF* CF = static_cast<TF*>(a.CF);
+  TF* G = static_cast<TF*>(a.G);
   const double* U = a.U + 4 * cs.cell_off;
   const double cfl = a.ctl[grp.cs].cfl;
   double cprev[16];
@@ -265,19 +276,30 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
       D[10] += dg;
       D[15] += dg;
     }
-    // pivot block: den = D - A c_prev with A = -JJL(j)
-    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, T1);
+    // pivot block den = D - A c_prev with A = -JJL(j); inv = den^-1
+    double A[16];
+    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        double s = T1[r * 4 + 0] * cprev[0 * 4 + c];
+        double s = A[r * 4 + 0] * cprev[0 * 4 + c];
 #pragma unroll
-        for (int k = 1; k < 4; ++k) s += T1[r * 4 + k] * cprev[k * 4 + c];
+        for (int k = 1; k < 4; ++k) s += A[r * 4 + k] * cprev[k * 4 + c];
         D[r * 4 + c] = D[r * 4 + c] + s;
       }
     double inv[16];
     inv4(D, inv);
+    // G = inv * JJL(j) = -inv A: the forward recurrence becomes d_j = inv r_j + G d_{j-1}
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        double s = inv[r * 4 + 0] * A[0 * 4 + c];
+#pragma unroll
+        for (int k = 1; k < 4; ++k) s += inv[r * 4 + k] * A[k * 4 + c];
+        D[r * 4 + c] = s;
+      }
     load_block(JJR, cs.rows_nc1, nc + 1, grp.g, j + 1, lane, T1);
 #pragma unroll
     for (int r = 0; r < 4; ++r)
@@ -290,14 +312,129 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
       }
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
-      a.INV[lbidx(cs.rows_nc, nc, grp.g, j, e, lane)] = inv[e];
-      a.CF[lbidx(cs.rows_nc, nc, grp.g, j, e, lane)] = cprev[e];
+      const size_t q = lbidx(cs.rows_nc, nc, grp.g, j, e, lane);
+      INV[q] = TF(inv[e]);
+      CF[q] = TF(cprev[e]);
+      G[q] = TF(D[e]);
     }
   }
 }
 
-template <typename TJ>
-__global__ void __launch_bounds__(128) k_sweep(Batch b, SweepArgs a) {
+// ---------------------------------------------------------------------------
+// right-hand side of one line-Jacobi sweep, fully parallel over cells:
+//   e = inv_j (r - off),  off = Bim x[i-1] + Bip x[i+1] = -(JIL x[i-1]) + JIR(i+1) x[i+1]
+// (off = 0 on the first sweep).  One thread per cell, 32 x 8 cells per CTA.
+// ---------------------------------------------------------------------------
+template <typename TJ, typename TF>
+__global__ void __launch_bounds__(256) k_rhs(Batch b, RhsArgs a) {
+  const Tile t = b.tiles[blockIdx.x];
+  if (!case_live(b, t.cs, a.need)) return;
+  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
+  if (lane >= t.ti || row >= t.tj) return;
+  const CaseDev& cs = b.cases[t.cs];
+  const GridDev& g = cs.g;
+  const int ni = g.ni, nc = g.nc;
+  const int i = t.i0 + lane, j = t.j0 + row, grp = t.i0 / kLanes;
+  const size_t base = 4 * cs.cell_off;
+  double rhs[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) rhs[k] = a.r[base + vidx(g, k, j, i)];
+  if (a.xprev != nullptr) {
+    const int ip = (i + 1 == ni) ? 0 : i + 1;
+    const int im = (i == 0) ? ni - 1 : i - 1;
+    const double* xp = a.xprev + base;
+    double xm4[4], xp4[4], AL[16], AR[16];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      xm4[k] = xp[vidx(g, k, j, im)];
+      xp4[k] = xp[vidx(g, k, j, ip)];
+    }
+    load_block(static_cast<const TJ*>(a.JIL), cs.rows_nc, nc, grp, j, lane, AL);
+    load_block(static_cast<const TJ*>(a.JIR), cs.rows_nc, nc, ip / kLanes, j, ip % kLanes, AR);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double s1 = AL[q * 4 + 0] * xm4[0];
+      double s2 = AR[q * 4 + 0] * xp4[0];
+#pragma unroll
+      for (int k = 1; k < 4; ++k) {
+        s1 += AL[q * 4 + k] * xm4[k];
+        s2 += AR[q * 4 + k] * xp4[k];
+      }
+      rhs[q] = rhs[q] - (-s1 + s2);
+    }
+  }
+  double IV[16];
+  load_block(static_cast<const TF*>(a.INV), cs.rows_nc, nc, grp, j, lane, IV);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double s = IV[q * 4 + 0] * rhs[0];
+#pragma unroll
+    for (int k = 1; k < 4; ++k) s += IV[q * 4 + k] * rhs[k];
+    a.out[base + vidx(g, q, j, i)] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the sequential part of the block-Thomas solve, in place on x:
+//   forward   d_j = e_j + G_j d_{j-1}
+//   backward  x_j = d_j - C_j x_{j+1}
+// one thread per line; the operands of the next 4 steps are loaded ahead so
+// each step waits on a quarter of the memory latency
+// ---------------------------------------------------------------------------
+template <typename TF>
+struct StepBuf {
+  double v[4];
+  TF M[16];
+};
+
+template <typename TF>
+__device__ __forceinline__ void load_step(StepBuf<TF>& s, const double* x, const TF* M, const CaseDev& cs,
+                                          const GridDev& g, int grp, int lane, int i, int j) {
+  if (j < 0 || j >= g.nc) return;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s.v[k] = x[vidx(g, k, j, i)];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) s.M[e] = M[lbidx(cs.rows_nc, g.nc, grp, j, e, lane)];
+}
+
+template <typename TF>
+__device__ __forceinline__ void fwd_step(const StepBuf<TF>& s, double d[4], double* x, const GridDev& g, int i,
+                                         int j) {
+  double nd[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double acc = s.v[q];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc += (double)s.M[q * 4 + k] * d[k];
+    nd[q] = acc;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    d[q] = nd[q];
+    x[vidx(g, q, j, i)] = nd[q];
+  }
+}
+
+template <typename TF>
+__device__ __forceinline__ void bwd_step(const StepBuf<TF>& s, double xn[4], double* x, const GridDev& g, int i,
+                                         int j) {
+  double nx[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc += (double)s.M[q * 4 + k] * xn[k];
+    nx[q] = s.v[q] - acc;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    xn[q] = nx[q];
+    x[vidx(g, q, j, i)] = nx[q];
+  }
+}
+
+template <typename TF>
+__global__ void __launch_bounds__(128) k_lines(Batch b, LinesArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gid = blockIdx.x * 4 + warp;
   if (gid >= b.ngroups) return;
@@ -306,88 +443,53 @@ __global__ void __launch_bounds__(128) k_sweep(Batch b, SweepArgs a) {
   if (lane >= grp.n) return;
   const CaseDev& cs = b.cases[grp.cs];
   const GridDev& g = cs.g;
-  const int ni = g.ni, nc = g.nc;
+  const int nc = g.nc;
   const int i = grp.i0 + lane;
-  const int ip = (i + 1 == ni) ? 0 : i + 1;
-  const int im = (i == 0) ? ni - 1 : i - 1;
-  const int gp = ip / kLanes, lp = ip % kLanes;
-  const TJ* JIL = static_cast<const TJ*>(a.JIL);
-  const TJ* JIR = static_cast<const TJ*>(a.JIR);
-  const TJ* JJL = static_cast<const TJ*>(a.JJL);
-  const size_t base = 4 * cs.cell_off;
-  const double* r = a.r + base;
-  const double* xp = a.xprev ? a.xprev + base : nullptr;
-  double* out = a.out + base;
-  double dprev[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int j = 0; j < nc; ++j) {
-    double rhs[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) rhs[k] = r[vidx(g, k, j, i)];
-    if (xp != nullptr) {
-      double xm4[4], xp4[4], off[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        xm4[k] = xp[vidx(g, k, j, im)];
-        xp4[k] = xp[vidx(g, k, j, ip)];
-      }
-      double AL[16], AR[16];
-      load_block(JIL, cs.rows_nc, nc, grp.g, j, lane, AL);
-      load_block(JIR, cs.rows_nc, nc, gp, j, lp, AR);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        double s1 = AL[q * 4 + 0] * xm4[0];
-        double s2 = AR[q * 4 + 0] * xp4[0];
-#pragma unroll
-        for (int k = 1; k < 4; ++k) {
-          s1 += AL[q * 4 + k] * xm4[k];
-          s2 += AR[q * 4 + k] * xp4[k];
-        }
-        off[q] = -s1 + s2;
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) rhs[q] = rhs[q] - off[q];
+  double* x = a.x + 4 * cs.cell_off;
+  const TF* G = static_cast<const TF*>(a.G);
+  const TF* CF = static_cast<const TF*>(a.CF);
+  StepBuf<TF> b0, b1, b2, b3;
+  double d[4] = {0.0, 0.0, 0.0, 0.0};
+  load_step(b0, x, G, cs, g, grp.g, lane, i, 0);
+  load_step(b1, x, G, cs, g, grp.g, lane, i, 1);
+  load_step(b2, x, G, cs, g, grp.g, lane, i, 2);
+  load_step(b3, x, G, cs, g, grp.g, lane, i, 3);
+  for (int j = 0; j < nc; j += 4) {
+    fwd_step(b0, d, x, g, i, j);
+    load_step(b0, x, G, cs, g, grp.g, lane, i, j + 4);
+    if (j + 1 < nc) {
+      fwd_step(b1, d, x, g, i, j + 1);
+      load_step(b1, x, G, cs, g, grp.g, lane, i, j + 5);
     }
-    double A[16], IV[16];
-    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
-#pragma unroll
-    for (int e = 0; e < 16; ++e) IV[e] = a.INV[lbidx(cs.rows_nc, nc, grp.g, j, e, lane)];
-    double tv[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      double s = A[q * 4 + 0] * dprev[0];
-#pragma unroll
-      for (int k = 1; k < 4; ++k) s += A[q * 4 + k] * dprev[k];
-      tv[q] = rhs[q] + s;
+    if (j + 2 < nc) {
+      fwd_step(b2, d, x, g, i, j + 2);
+      load_step(b2, x, G, cs, g, grp.g, lane, i, j + 6);
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      double s = IV[q * 4 + 0] * tv[0];
-#pragma unroll
-      for (int k = 1; k < 4; ++k) s += IV[q * 4 + k] * tv[k];
-      dprev[q] = s;
+    if (j + 3 < nc) {
+      fwd_step(b3, d, x, g, i, j + 3);
+      load_step(b3, x, G, cs, g, grp.g, lane, i, j + 7);
     }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) out[vidx(g, k, j, i)] = dprev[k];
   }
   double xn[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int j = nc - 1; j >= 0; --j) {
-    double C[16], d[4];
-#pragma unroll
-    for (int e = 0; e < 16; ++e) C[e] = a.CF[lbidx(cs.rows_nc, nc, grp.g, j, e, lane)];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) d[k] = out[vidx(g, k, j, i)];
-    double x[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      double s = C[q * 4 + 0] * xn[0];
-#pragma unroll
-      for (int k = 1; k < 4; ++k) s += C[q * 4 + k] * xn[k];
-      x[q] = d[q] - s;
+  const int top = nc - 1;
+  load_step(b0, x, CF, cs, g, grp.g, lane, i, top);
+  load_step(b1, x, CF, cs, g, grp.g, lane, i, top - 1);
+  load_step(b2, x, CF, cs, g, grp.g, lane, i, top - 2);
+  load_step(b3, x, CF, cs, g, grp.g, lane, i, top - 3);
+  for (int j = top; j >= 0; j -= 4) {
+    bwd_step(b0, xn, x, g, i, j);
+    load_step(b0, x, CF, cs, g, grp.g, lane, i, j - 4);
+    if (j - 1 >= 0) {
+      bwd_step(b1, xn, x, g, i, j - 1);
+      load_step(b1, x, CF, cs, g, grp.g, lane, i, j - 5);
     }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      out[vidx(g, k, j, i)] = x[k];
-      xn[k] = x[k];
+    if (j - 2 >= 0) {
+      bwd_step(b2, xn, x, g, i, j - 2);
+      load_step(b2, x, CF, cs, g, grp.g, lane, i, j - 6);
+    }
+    if (j - 3 >= 0) {
+      bwd_step(b3, xn, x, g, i, j - 3);
+      load_step(b3, x, CF, cs, g, grp.g, lane, i, j - 7);
     }
   }
 }
@@ -397,22 +499,29 @@ void launch_face_jac(const Batch& b, const JacArgs& a, cudaStream_t s) {
   if (b.ntiles == 0) return;
   k_face_jac<T><<<b.ntiles, 256, 0, s>>>(b, a);
 }
-template <typename TJ>
+template <typename TJ, typename TF>
 void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s) {
   if (b.ngroups == 0) return;
-  k_factor<TJ><<<(b.ngroups + 3) / 4, 128, 0, s>>>(b, a);
+  k_factor<TJ, TF><<<(b.ngroups + 3) / 4, 128, 0, s>>>(b, a);
 }
-template <typename TJ>
-void launch_sweep(const Batch& b, const SweepArgs& a, cudaStream_t s) {
+template <typename TJ, typename TF>
+void launch_rhs(const Batch& b, const RhsArgs& a, cudaStream_t s) {
+  if (b.ntiles == 0) return;
+  k_rhs<TJ, TF><<<b.ntiles, 256, 0, s>>>(b, a);
+}
+template <typename TF>
+void launch_lines(const Batch& b, const LinesArgs& a, cudaStream_t s) {
   if (b.ngroups == 0) return;
-  k_sweep<TJ><<<(b.ngroups + 3) / 4, 128, 0, s>>>(b, a);
+  k_lines<TF><<<(b.ngroups + 3) / 4, 128, 0, s>>>(b, a);
 }
 
 template void launch_face_jac<double>(const Batch&, const JacArgs&, cudaStream_t);
 template void launch_face_jac<float>(const Batch&, const JacArgs&, cudaStream_t);
-template void launch_factor<double>(const Batch&, const FactorArgs&, cudaStream_t);
-template void launch_factor<float>(const Batch&, const FactorArgs&, cudaStream_t);
-template void launch_sweep<double>(const Batch&, const SweepArgs&, cudaStream_t);
-template void launch_sweep<float>(const Batch&, const SweepArgs&, cudaStream_t);
+template void launch_factor<double, double>(const Batch&, const FactorArgs&, cudaStream_t);
+template void launch_factor<float, float>(const Batch&, const FactorArgs&, cudaStream_t);
+template void launch_rhs<double, double>(const Batch&, const RhsArgs&, cudaStream_t);
+template void launch_rhs<float, float>(const Batch&, const RhsArgs&, cudaStream_t);
+template void launch_lines<double>(const Batch&, const LinesArgs&, cudaStream_t);
+template void launch_lines<float>(const Batch&, const LinesArgs&, cudaStream_t);
 
 }  // namespace a2d

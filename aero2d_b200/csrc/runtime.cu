@@ -105,7 +105,7 @@ struct a2d_plan {
   // workspace layout (offsets)
   size_t o_cases = 0, o_tiles = 0, o_chunks = 0, o_groups = 0, o_cpoff = 0, o_live = 0, o_ctl = 0;
   size_t o_vec[kNumVec] = {};
-  size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_V = 0;
+  size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_G = 0, o_V = 0;
   size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_y = 0, o_lsq = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
   size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0;
   int pstride = 0;
@@ -116,6 +116,7 @@ struct a2d_plan {
   cudaStream_t graph_stream = nullptr;
   int* host_count = nullptr;
   int steps_taken = 0;
+  int kernels_per_step = 0;
 
   template <typename X> X* at(size_t off) const { return reinterpret_cast<X*>(ws + off); }
   double* vec(int s) const { return at<double>(o_vec[s]); }
@@ -187,8 +188,9 @@ static void layout(a2d_plan* P) {
   P->o_JIR = cv.take(P->tj * lb * P->rows_nc);
   P->o_JJL = cv.take(P->tj * lb * P->rows_nc1);
   P->o_JJR = cv.take(P->tj * lb * P->rows_nc1);
-  P->o_INV = cv.take(8 * lb * P->rows_nc);
-  P->o_CF = cv.take(8 * lb * P->rows_nc);
+  P->o_INV = cv.take(P->tj * lb * P->rows_nc);
+  P->o_CF = cv.take(P->tj * lb * P->rows_nc);
+  P->o_G = cv.take(P->tj * lb * P->rows_nc);
   P->o_V = cv.take(P->tb * 4 * C * (size_t)(P->m + 1));
   P->o_H = cv.take(8 * (size_t)B * kMaxRestart * (kMaxRestart + 1));
   P->o_h1 = cv.take(8 * (size_t)B * (kMaxRestart + 1));
@@ -294,22 +296,26 @@ namespace a2d {
 
 template <typename TJ>
 static void precond(a2d_plan* P, const Batch& B, const double* rin, double* dst, uint32_t need, cudaStream_t s) {
-  SweepArgs a;
-  a.INV = P->at<double>(P->o_INV);
-  a.CF = P->at<double>(P->o_CF);
-  a.JJL = P->at<void>(P->o_JJL);
-  a.JIL = P->at<void>(P->o_JIL);
-  a.JIR = P->at<void>(P->o_JIR);
-  a.need = need;
-  a.r = rin;
+  RhsArgs ra;
+  ra.r = rin;
+  ra.INV = P->at<void>(P->o_INV);
+  ra.JIL = P->at<void>(P->o_JIL);
+  ra.JIR = P->at<void>(P->o_JIR);
+  ra.need = need;
+  LinesArgs la;
+  la.G = P->at<void>(P->o_G);
+  la.CF = P->at<void>(P->o_CF);
+  la.need = need;
   const int sweeps = std::max(1, P->p.jacobi_sweeps);
   double* bufs[2] = {P->vec(kPA), P->vec(kPB)};
   const double* prev = nullptr;
   for (int sw = 0; sw < sweeps; ++sw) {
     double* out = (sw == sweeps - 1) ? dst : bufs[sw & 1];
-    a.xprev = prev;
-    a.out = out;
-    launch_sweep<TJ>(B, a, s);
+    ra.xprev = prev;
+    ra.out = out;
+    launch_rhs<TJ, TJ>(B, ra, s);
+    la.x = out;
+    launch_lines<TJ>(B, la, s);
     prev = out;
   }
 }
@@ -333,12 +339,13 @@ static void precond_setup(a2d_plan* P, const Batch& B, uint32_t need, cudaStream
   fa.JIR = ja.JIR;
   fa.JJL = ja.JJL;
   fa.JJR = ja.JJR;
-  fa.INV = P->at<double>(P->o_INV);
-  fa.CF = P->at<double>(P->o_CF);
+  fa.INV = P->at<void>(P->o_INV);
+  fa.CF = P->at<void>(P->o_CF);
+  fa.G = P->at<void>(P->o_G);
   fa.diag = P->at<double>(P->o_diag);
   fa.cfl_base = P->p.cfl;
   fa.need = need;
-  launch_factor<TJ>(B, fa, s);
+  launch_factor<TJ, TJ>(B, fa, s);
 }
 
 static StencilArgs<double> residual_args(a2d_plan* P) {
@@ -507,6 +514,18 @@ static int newton_step(a2d_plan* P, cudaStream_t s) {
     cudaError_t e = cudaStreamEndCapture(cap, &g);
     cudaStreamDestroy(cap);
     if (e != cudaSuccess) return fail(A2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    size_t nn = 0;
+    if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+      std::vector<cudaGraphNode_t> nodes(nn);
+      if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess) {
+        int nk = 0;
+        for (size_t q = 0; q < nn; ++q) {
+          cudaGraphNodeType ty;
+          if (cudaGraphNodeGetType(nodes[q], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++nk;
+        }
+        P->kernels_per_step = nk;
+      }
+    }
     e = cudaGraphInstantiate(&P->graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(A2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
@@ -805,6 +824,192 @@ int a2d_newton_run(a2d_plan* P, int max_steps, int* steps, void* stream) {
     if (*P->host_count == 0) break;
   }
   if (steps != nullptr) *steps = done;
+  return A2D_OK;
+}
+
+int a2d_live_count(a2d_plan* P, int* n, void* stream) {
+  A2D_BOUND(P);
+  if (n == nullptr) return fail(A2D_ERR_ARG, "null output");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int* dcount = P->at<int>(P->o_cnt);
+  k_count<<<1, 256, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.retire, dcount);
+  A2D_CK(cudaMemcpyAsync(P->host_count, dcount, sizeof(int), cudaMemcpyDeviceToHost, s));
+  A2D_CK(cudaStreamSynchronize(s));
+  *n = *P->host_count;
+  return A2D_OK;
+}
+
+int a2d_plan_stats(const a2d_plan* P, int* kernels_per_step, int* steps_taken, size_t* table_bytes) {
+  if (P == nullptr) return fail(A2D_ERR_ARG, "null plan");
+  if (kernels_per_step) *kernels_per_step = P->kernels_per_step;
+  if (steps_taken) *steps_taken = P->steps_taken;
+  if (table_bytes)
+    *table_bytes = sizeof(CaseDev) * P->ncases + sizeof(Tile) * P->tiles.size() + sizeof(Chunk) * P->chunks.size() +
+                   sizeof(Group) * P->groups.size() + sizeof(long long) * P->ncases;
+  return A2D_OK;
+}
+
+int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
+  A2D_BOUND(P);
+  if (ms == nullptr || reps < 1) return fail(A2D_ERR_ARG, "time_kernel: bad arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Batch B = P->batch;
+  B.live = nullptr;
+  const bool mixed = P->p.precision == A2D_MIXED;
+  const size_t vs = 4 * (size_t)P->C;
+  const int half = std::max(1, P->m / 2);
+  auto launch_once = [&]() {
+    switch (which) {
+      case A2D_K_JVP: {
+        if (mixed) {
+          StencilArgs<float> a;
+          a.U = P->vec(kU);
+          a.V = P->at<float>(P->o_V);
+          a.diag = P->at<double>(P->o_diag);
+          a.out = P->vec(kZ);
+          a.lim_k = P->p.lim_k;
+          a.order = P->p.order;
+          a.vortex = P->p.vortex_correction;
+          launch_stencil<float, true, float>(B, a, s);
+        } else {
+          StencilArgs<double> a = residual_args(P);
+          a.V = P->at<double>(P->o_V);
+          a.diag = P->at<double>(P->o_diag);
+          a.out = P->vec(kZ);
+          launch_stencil<double, true, double>(B, a, s);
+        }
+        break;
+      }
+      case A2D_K_LINES: {
+        LinesArgs la;
+        la.G = P->at<void>(P->o_G);
+        la.CF = P->at<void>(P->o_CF);
+        la.x = P->vec(kPA);
+        if (mixed) launch_lines<float>(B, la, s);
+        else launch_lines<double>(B, la, s);
+        break;
+      }
+      case A2D_K_RHS: {
+        RhsArgs ra;
+        ra.r = P->vec(kZ);
+        ra.xprev = P->vec(kPB);
+        ra.out = P->vec(kPA);
+        ra.INV = P->at<void>(P->o_INV);
+        ra.JIL = P->at<void>(P->o_JIL);
+        ra.JIR = P->at<void>(P->o_JIR);
+        if (mixed) launch_rhs<float, float>(B, ra, s);
+        else launch_rhs<double, double>(B, ra, s);
+        break;
+      }
+      case A2D_K_DOTS: {
+        if (mixed) {
+          DotArgs<float> d;
+          d.w = P->vec(kW);
+          d.V = P->at<float>(P->o_V);
+          d.vstride = vs;
+          d.nq = half;
+          d.with_norm = 1;
+          d.part = P->at<double>(P->o_cpart);
+          d.pstride = P->pstride;
+          launch_dots<float>(B, d, s);
+        } else {
+          DotArgs<double> d;
+          d.w = P->vec(kW);
+          d.V = P->at<double>(P->o_V);
+          d.vstride = vs;
+          d.nq = half;
+          d.with_norm = 1;
+          d.part = P->at<double>(P->o_cpart);
+          d.pstride = P->pstride;
+          launch_dots<double>(B, d, s);
+        }
+        break;
+      }
+      case A2D_K_UPDATE: {
+        if (mixed) {
+          UpdateArgs<float> u;
+          u.w = P->vec(kPA);
+          u.V = P->at<float>(P->o_V);
+          u.vstride = vs;
+          u.nq = half;
+          u.part = P->at<double>(P->o_cpart);
+          u.pstride = P->pstride;
+          u.hstore = P->at<double>(P->o_h1);
+          u.part_norm = P->at<double>(P->o_cpartn);
+          launch_update<float>(B, u, s);
+        } else {
+          UpdateArgs<double> u;
+          u.w = P->vec(kPA);
+          u.V = P->at<double>(P->o_V);
+          u.vstride = vs;
+          u.nq = half;
+          u.part = P->at<double>(P->o_cpart);
+          u.pstride = P->pstride;
+          u.hstore = P->at<double>(P->o_h1);
+          u.part_norm = P->at<double>(P->o_cpartn);
+          launch_update<double>(B, u, s);
+        }
+        break;
+      }
+      case A2D_K_RESIDUAL: {
+        StencilArgs<double> a = residual_args(P);
+        a.out = P->vec(kPA);
+        a.sign = -1.0;
+        a.circ_out = P->at<double>(P->o_circ);
+        a.tile_part = P->at<double>(P->o_tpart);
+        launch_stencil<double, false, double>(B, a, s);
+        break;
+      }
+      case A2D_K_FACEJAC:
+      case A2D_K_FACTOR: {
+        JacArgs ja;
+        ja.U = P->vec(kU);
+        ja.circ = P->at<double>(P->o_circ);
+        ja.JIL = P->at<void>(P->o_JIL);
+        ja.JIR = P->at<void>(P->o_JIR);
+        ja.JJL = P->at<void>(P->o_JJL);
+        ja.JJR = P->at<void>(P->o_JJR);
+        ja.vortex = P->p.vortex_correction;
+        if (which == A2D_K_FACEJAC) {
+          if (mixed) launch_face_jac<float>(B, ja, s);
+          else launch_face_jac<double>(B, ja, s);
+        } else {
+          FactorArgs fa;
+          fa.U = P->vec(kU);
+          fa.ctl = P->ctl();
+          fa.JIL = ja.JIL;
+          fa.JIR = ja.JIR;
+          fa.JJL = ja.JJL;
+          fa.JJR = ja.JJR;
+          fa.INV = P->at<void>(P->o_INV);
+          fa.CF = P->at<void>(P->o_CF);
+          fa.G = P->at<void>(P->o_G);
+          fa.diag = P->at<double>(P->o_diag);
+          fa.cfl_base = P->p.cfl;
+          if (mixed) launch_factor<float, float>(B, fa, s);
+          else launch_factor<double, double>(B, fa, s);
+        }
+        break;
+      }
+      default:
+        break;
+    }
+  };
+  if (which < 0 || which > A2D_K_FACTOR) return fail(A2D_ERR_ARG, "time_kernel: unknown kernel");
+  cudaEvent_t e0, e1;
+  A2D_CK(cudaEventCreate(&e0));
+  A2D_CK(cudaEventCreate(&e1));
+  launch_once();   // warm-up launch
+  A2D_CK(cudaEventRecord(e0, s));
+  for (int q = 0; q < reps; ++q) launch_once();
+  A2D_CK(cudaEventRecord(e1, s));
+  A2D_CK(cudaEventSynchronize(e1));
+  float t = 0.f;
+  A2D_CK(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  A2D_CK(cudaGetLastError());
+  *ms = t / reps;
   return A2D_OK;
 }
 

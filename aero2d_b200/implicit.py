@@ -130,6 +130,7 @@ class ImplicitEuler:
                 cl_h[nsteps[k]:, k] = cl_h[nsteps[k] - 1, k]
         self.cl_history = cl_h
         self.frozen = frozen
+        self.done = done
         self.steps_taken = nsteps
         coef, cps = pl.forces()
         c = coef.cpu().numpy()

@@ -171,6 +171,29 @@ class Plan:
         self.call("a2d_newton_run", int(max_steps), C.byref(n))
         return n.value
 
+    def live_count(self) -> int:
+        n = C.c_int()
+        self.call("a2d_live_count", C.byref(n))
+        return n.value
+
+    def stats(self):
+        """(kernel launches per Newton step, Newton steps since reset)."""
+        k, s = C.c_int(), C.c_int()
+        _lib.check(self.lib.a2d_plan_stats(self.handle, C.byref(k), C.byref(s), None))
+        return k.value, s.value
+
+    def table_bytes(self) -> int:
+        """Bytes of the case tables copied to the device at bind time."""
+        n = C.c_size_t()
+        _lib.check(self.lib.a2d_plan_stats(self.handle, None, None, C.byref(n)))
+        return n.value
+
+    def time_kernel(self, which: int, reps: int = 20) -> float:
+        """Mean milliseconds per launch of one kernel on the plan's data (CUDA events)."""
+        ms = C.c_float()
+        self.call("a2d_time_kernel", int(which), int(reps), C.byref(ms))
+        return float(ms.value)
+
     def status(self):
         B = self.B
         nsteps = (C.c_int * B)()

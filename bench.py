@@ -1,0 +1,460 @@
+#!/usr/bin/env python
+"""Benchmark of the batched Euler Newton-Krylov path on B200.
+
+Workload (one "step" = one batch solve): 64 Euler cases on one shared 256 x 64
+O-grid of NACA 2412 (ogrid(naca4("2412", 129), nj=65, ds0=2e-3, radius=20)),
+M ~ U[0.30, 0.75] and alpha ~ U[-4, 8] deg from default_rng(2412), every case
+its own state in one batched plan, pseudo-transient Newton-Krylov (GMRES
+restart 30, 4 line-Jacobi sweeps, reference defaults otherwise) from the
+freestream to a residual drop of 1e-10 (at most 200 Newton steps).  Inputs are
+synthetic (seeded), like the reference's own benchmark inputs.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line.  `value` is converged cases per second of the
+mixed-precision batch solve with grid and plan resident in HBM; `e2e` is the
+same metric through the public API (ImplicitEuler.solve with host arrays in and
+host results out).  Under torchrun every rank solves its own 64-case batch
+(seed 2412 + rank, weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "converged Euler cases/sec + p50/p99 latency, mixed vs plain FP64 on 1 B200 at |ΔCl|≤1e-4"
+GRID = dict(code="2412", n_side=129, nj=65, ds0=2e-3, radius=20.0)
+CASES = 64
+MACH = (0.30, 0.75)
+ALPHA = (-4.0, 8.0)
+SEED = 2412
+TOL = 1e-10
+RESTART = 30
+MAX_ITER = 200
+# Newton steps per converged case of this workload, FP64, as measured by the
+# CUDA path (which follows the oracle step for step); converts the reference
+# arm's timed Newton steps into converged cases per second.
+NEWTON_STEPS_PER_CASE = 145.5
+
+
+def draw_cases(seed: int, n: int):
+    rng = np.random.default_rng(seed)
+    machs = rng.uniform(MACH[0], MACH[1], n)
+    alphas = rng.uniform(ALPHA[0], ALPHA[1], n)
+    return machs, alphas
+
+
+def make_grid():
+    from aero2d_b200.geometry import naca4
+    from aero2d_b200.grid import ogrid
+    return ogrid(naca4(GRID["code"], GRID["n_side"]), nj=GRID["nj"], ds0=GRID["ds0"], radius=GRID["radius"])
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 oracle (NumPy restatement of aero2d/euler.py and
+# aero2d/implicit.py), one Newton step per process
+# ---------------------------------------------------------------------------
+def _oracle_newton_step(args):
+    k, seed = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, str(ROOT))
+    from oracle.euler_oracle import EulerModel
+    from oracle.implicit_oracle import ImplicitModel
+    g = make_grid()
+    machs, alphas = draw_cases(seed, CASES)
+    im = ImplicitModel(EulerModel(g.x, g.y), gmres_restart=RESTART)
+    w = im.b.freestream(machs[k], alphas[k])
+    U = im.b.init_state(w)
+    t = time.perf_counter()
+    im.step(U, w, im.cfl0)
+    return time.perf_counter() - t
+
+
+def cpu_oracle_rate(procs: int, seed: int = SEED):
+    """Converged cases/s of the oracle on `procs` host processes, from one
+    timed Newton step per process (BLAS threads 1 per process)."""
+    import multiprocessing as mp
+    os.environ["OMP_NUM_THREADS"] = "1"
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        t0 = time.perf_counter()
+        step_times = pool.map(_oracle_newton_step, [(k % CASES, seed) for k in range(procs)])
+        wall = time.perf_counter() - t0
+    per_step = statistics.mean(step_times)
+    rate = procs / per_step / NEWTON_STEPS_PER_CASE
+    return rate, per_step, wall
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = [ln.split(",") for ln in open(self.file.name).read().splitlines() if ln.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        busy = [v for v in sm if v > 0.5 * (smax or max(sm))] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------
+def batch_solve(plan, max_iter):
+    """One batch solve from the freestream; CUDA events after every Newton step.
+    Returns (elapsed_ms, per-case latency ms, nsteps, converged, frozen)."""
+    import torch
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    plan.init_freestream()
+    evs = []
+    for _ in range(max_iter):
+        plan.newton_step()
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        evs.append(e)
+        if plan.live_count() == 0:
+            break
+    evs[-1].synchronize()
+    t_steps = np.array([ev0.elapsed_time(e) for e in evs])
+    nsteps, done, frozen, lastrn, r0 = plan.status()
+    conv = done & ~frozen
+    lat = np.array([t_steps[n - 1] if n > 0 else 0.0 for n in nsteps])
+    return float(t_steps[-1]), lat, nsteps, conv, frozen, len(evs)
+
+
+def algorithmic_bytes(kernel: str, cells: int, restart: int, mixed: bool) -> float:
+    """Bytes a kernel must move per launch for the whole batch (cells = total
+    cells); counts the matrix and vector words of the kernel's definition once."""
+    f = 4 if mixed else 8
+    d = 8
+    half = max(1, restart // 2)
+    per_cell = {
+        # e, G, d(store), d(load), CF, x(store)
+        "lines": 4 * d + 16 * f + 4 * d + 4 * d + 16 * f + 4 * d,
+        # r, x_prev, JIL, JIR, INV, e
+        "rhs": 4 * d + 4 * d + 16 * f + 16 * f + 16 * f + 4 * d,
+        # U, V, diag, z, face vectors (2 i-face + 2 j-face components)
+        "jvp": 4 * d + 4 * f + d + 4 * d + 4 * f,
+        # w, restart/2 basis vectors
+        "dots": 4 * d + half * 4 * f,
+        # w (load + store), restart/2 basis vectors
+        "update": 8 * d + half * 4 * f,
+    }[kernel]
+    return float(per_cell) * cells
+
+
+def launches_per_step(kernel: str, restart: int, sweeps: int = 4) -> int:
+    napp = restart + 2
+    return {"lines": sweeps * napp, "rhs": (sweeps - 1) * napp, "jvp": restart + 1,
+            "dots": 2 * restart, "update": 2 * restart}[kernel]
+
+
+def read_traffic(kernel: str):
+    """DRAM bytes per cell of a kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "dram_traffic.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        parts = ln.split()
+        if len(parts) >= 2 and parts[0] == kernel and not ln.startswith("#"):
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.load(open(p))["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def gpu_arm(args, rank: int, world: int, dist):
+    import torch
+    from aero2d_b200 import _lib
+    from aero2d_b200.euler import EulerSolver
+    from aero2d_b200.implicit import ImplicitEuler
+    from aero2d_b200.plan import Plan
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    B = args.cases
+    seed = SEED + rank
+    machs, alphas = draw_cases(seed, B)
+    grid = make_grid()
+
+    def make_plan(dtype, cases_m, cases_a):
+        base = EulerSolver(grid, dtype=dtype, device=dev)
+        s = ImplicitEuler(base, gmres_restart=args.restart)
+        winf = base.freestream(cases_m, cases_a)
+        return Plan([base.dgrid] * len(cases_m), winf, s.params(args.tol, args.max_iter), dev), base
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- headline: mixed-precision batch solve, device resident ------------
+    plan, base = make_plan(np.float32, machs, alphas)
+    for _ in range(args.warmup):
+        batch_solve(plan, args.max_iter)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    t0 = time.perf_counter()
+    runs = [batch_solve(plan, args.max_iter) for _ in range(args.steps)]
+    barrier()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    elapsed_ms = sum(r[0] for r in runs)
+    converged = sum(int(r[3].sum()) for r in runs)
+    kps, _ = plan.stats()
+    launches = sum(r[5] * (kps + 1) + 2 for r in runs)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        c = torch.tensor([float(converged)], dtype=torch.float64, device=dev)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        elapsed_ms, converged = float(t.item()), int(c.item())
+    lat = np.concatenate([r[1][r[3]] for r in runs]) if converged else np.array([np.nan])
+    nsteps_mix = runs[-1][2]
+    coef_mix = plan.forces()[0].cpu().numpy()
+    conv_mix = runs[-1][3]
+    value = converged / (elapsed_ms / 1e3)
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "cases/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
+        "data": "synthetic (seeded NACA 2412 cases; random (M, alpha) per case)",
+        "config": {"workload": f"{B} cases on one 256x64 O-grid of NACA 2412, M~U[0.30,0.75], alpha~U[-4,8] deg, "
+                               f"seed {SEED}+rank, Newton-Krylov to residual drop {args.tol:g}",
+                   "cases_per_gpu": B, "grid": "256x64 (ogrid naca4('2412',129), nj=65, ds0=2e-3, radius=20)",
+                   "gmres_restart": args.restart, "jacobi_sweeps": 4, "max_newton_steps": args.max_iter,
+                   "precision": "mixed: FP64 residual/factorisation/Gram-Schmidt/update, FP32 JVP/face Jacobians/Krylov basis",
+                   "l2": "working set ~2 GB per batch, larger than the 126 MB L2 (no flush needed)",
+                   "parallelism": f"replicas x{world}, case sharding"},
+        "converged_cases": converged,
+        "cases_total": B * args.steps * world,
+        "newton_steps_mean": round(float(nsteps_mix.mean()), 2),
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 2), "p95": round(float(np.percentile(lat, 95)), 2),
+                       "p99": round(float(np.percentile(lat, 99)), 2),
+                       "note": "per converged case, from batch start to its retirement"},
+    }
+    if rank != 0:
+        return None
+
+    # ---- plain FP64 batch and the per-case FP64 path -----------------------
+    plan64, _ = make_plan(np.float64, machs, alphas)
+    batch_solve(plan64, args.max_iter)
+    r64 = batch_solve(plan64, args.max_iter)
+    coef64 = plan64.forces()[0].cpu().numpy()
+    conv64 = r64[3]
+    out["fp64_batched"] = {"value": round(int(conv64.sum()) / (r64[0] / 1e3), 3), "unit": "cases/s",
+                           "ms_per_batch": round(r64[0], 1), "newton_steps_mean": round(float(r64[2].mean()), 2)}
+    single, _ = make_plan(np.float64, machs[:1], alphas[:1])
+    batch_solve(single, args.max_iter)
+    t_single, n_single = 0.0, 0
+    for k in range(args.single_sample):
+        pk, _ = make_plan(np.float64, machs[k:k + 1], alphas[k:k + 1])
+        batch_solve(pk, 2)
+        r1 = batch_solve(pk, args.max_iter)
+        t_single += r1[0]
+        n_single += int(r1[3].sum())
+        del pk
+    per_case_rate = n_single / (t_single / 1e3) if n_single else 0.0
+    out["fp64_per_case"] = {"value": round(per_case_rate, 3), "unit": "cases/s",
+                            "sample": f"cases 0..{args.single_sample - 1} solved one at a time (B=1 plans)",
+                            "ratio_mixed_batched_over_this": round(value / per_case_rate, 2) if per_case_rate else None}
+    both = conv_mix & conv64
+    dcl = np.abs(coef_mix[:, 0] - coef64[:, 0])[both]
+    dcd = np.abs(coef_mix[:, 1] - coef64[:, 1])[both]
+    dcm = np.abs(coef_mix[:, 2] - coef64[:, 2])[both]
+    out["accuracy_vs_fp64"] = {"max_abs_dCl": float(dcl.max()) if both.any() else None,
+                               "max_abs_dCd": float(dcd.max()) if both.any() else None,
+                               "max_abs_dCm": float(dcm.max()) if both.any() else None,
+                               "cases_compared": int(both.sum()),
+                               "gate": "|dCl| <= 1e-4 and |dCd| <= 2e-6 against the FP64 path "
+                                       "(parity-pinned to the FP64 oracle)"}
+
+    # ---- roofline of the dominant kernel (CUDA events on the plan's stream) --
+    cells = B * 256 * 64
+    kernels = {"lines": _lib.K_LINES, "rhs": _lib.K_RHS, "jvp": _lib.K_JVP, "dots": _lib.K_DOTS,
+               "update": _lib.K_UPDATE}
+    ktimes = {k: plan.time_kernel(v, reps=20) for k, v in kernels.items()}
+    share = {k: ktimes[k] * launches_per_step(k, args.restart) for k in kernels}
+    dom = max(share, key=share.get)
+    peak, peak_kind = measured_peak()
+    achieved = algorithmic_bytes(dom, cells, args.restart, True) / (ktimes[dom] / 1e3) / 1e9
+    traffic_per_cell = read_traffic(dom)
+    out["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                       "unit": "GB/s", "frac": round(achieved / peak, 3), "peak_source": peak_kind,
+                       "traffic": (round(traffic_per_cell * cells) if traffic_per_cell else None),
+                       "algorithmic_bytes_per_launch": algorithmic_bytes(dom, cells, args.restart, True),
+                       "ms_per_launch": round(ktimes[dom], 4)}
+    out["kernels_ms_per_launch"] = {k: round(v, 4) for k, v in ktimes.items()}
+    out["kernels_ms_per_newton_step"] = {k: round(v, 3) for k, v in share.items()}
+
+    # ---- end to end through the public API ---------------------------------
+    def e2e_once():
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        s = ImplicitEuler(EulerSolver(grid, dtype=np.float32, device=dev), gmres_restart=args.restart)
+        r = s.solve(machs, alphas, n_iter=args.max_iter, tol=args.tol, verbose=False)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t, r, s
+    e2e_once()
+    te, r, s = e2e_once()
+    conv_e2e = int((s.done & ~s.frozen).sum())
+    ni, nj = grid.shape
+    h2d = 2 * ni * nj * 8 + B * 4 * 8 + plan.table_bytes()
+    d2h = (r.cl.nbytes + r.cd.nbytes + r.cm.nbytes + r.cp.nbytes + r.res_hist.nbytes
+           + s.cl_history.nbytes + B * (3 * 4 + 2 * 8))
+    out["e2e"] = {"value": round(conv_e2e / te, 3), "unit": "cases/s", "h2d_bytes_per_step": int(h2d),
+                  "d2h_bytes_per_step": int(d2h), "seconds": round(te, 3),
+                  "call": "ImplicitEuler(EulerSolver(grid, dtype=float32), gmres_restart=30).solve(machs, alphas, "
+                          "n_iter=200, tol=1e-10) with host arrays in and numpy results out"}
+    out["e2e"]["converged_cases"] = conv_e2e
+    out["gpu_launches"] = int(launches)
+    out["clocks"] = clk
+
+    # ---- CPU baseline ---------------------------------------------------------
+    if world == 1 and not args.no_cpu_baseline:
+        procs = max(1, min(os.cpu_count() or 1, args.cpu_procs))
+        rate, per_step, cpu_wall = cpu_oracle_rate(procs)
+        out["cpu_baseline"] = {"value": round(rate, 5), "unit": "cases/s", "cores": procs, "kind": "port",
+                               "sample": f"one Newton step (restart {RESTART}, 4 sweeps) of {procs} cases of this "
+                                         f"workload, one spawned process per case with one BLAS thread, "
+                                         f"{per_step:.2f} s per step; cases/s = processes / step time / "
+                                         f"{NEWTON_STEPS_PER_CASE} Newton steps per converged case",
+                               "wall_s": round(cpu_wall, 1)}
+    return out
+
+
+def reference_arm(args):
+    """The reference's CPU path: JAX is not installable here, so its FP64
+    NumPy restatement (oracle/) runs on all host cores."""
+    procs = max(1, os.cpu_count() or 1)
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        cpu_oracle_rate(procs)
+    vals, per = [], []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rate, per_step, _ = cpu_oracle_rate(procs)
+        vals.append(rate)
+        per.append(per_step)
+    wall = time.perf_counter() - t0
+    value = statistics.mean(vals)
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "cases/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic (seeded NACA 2412 cases)",
+            "config": {"workload": f"{CASES} cases on one 256x64 O-grid of NACA 2412, M~U[0.30,0.75], "
+                                   f"alpha~U[-4,8] deg, seed {SEED}, Newton-Krylov to residual drop {TOL:g}",
+                       "gmres_restart": RESTART},
+            "cpu_baseline": {"value": round(value, 5), "unit": "cases/s", "cores": procs, "kind": "port",
+                             "sample": f"per step: one Newton step of {procs} cases on {procs} spawned processes "
+                                       f"({statistics.mean(per):.2f} s per Newton step); the JAX reference "
+                                       "cannot be installed in this image (no jax wheel, no network)"},
+            "e2e": {"value": round(value, 5), "unit": "cases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--cases", type=int, default=CASES)
+    ap.add_argument("--restart", type=int, default=RESTART)
+    ap.add_argument("--tol", type=float, default=TOL)
+    ap.add_argument("--max-iter", type=int, default=MAX_ITER)
+    ap.add_argument("--single-sample", type=int, default=4)
+    ap.add_argument("--cpu-procs", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)))
+        return
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = td
+    try:
+        out = gpu_arm(args, rank, world, dist)
+        if rank == 0 and out is not None:
+            print(json.dumps(out))
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

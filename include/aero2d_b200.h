@@ -130,6 +130,27 @@ int a2d_case_scalars(const a2d_plan* plan, double* out, void* stream);
 /* per-step histories to host arrays [steps][ncases] (residual norm, Cl); steps <= max_iter */
 int a2d_history(const a2d_plan* plan, int steps, double* rn, double* cl, void* stream);
 
+/* number of cases still stepping (retire=1) or not yet done (retire=0); synchronises */
+int a2d_live_count(a2d_plan* plan, int* n, void* stream);
+/* kernel launches of one Newton step (counted in the captured graph; 0 before the
+ * first step), Newton steps taken since the last reset, and the bytes of the case
+ * tables that a2d_plan_bind copies to the device */
+int a2d_plan_stats(const a2d_plan* plan, int* kernels_per_step, int* steps_taken, size_t* table_bytes);
+
+/* ---- measurement ---- */
+#define A2D_K_JVP 0        /* linearised residual stencil on the whole batch            */
+#define A2D_K_LINES 1      /* sequential block-Thomas recurrences of one sweep          */
+#define A2D_K_RHS 2        /* parallel right-hand side of a coupled sweep               */
+#define A2D_K_DOTS 3       /* Gram-Schmidt projections against restart/2 basis vectors */
+#define A2D_K_UPDATE 4     /* Gram-Schmidt subtraction with restart/2 basis vectors     */
+#define A2D_K_RESIDUAL 5   /* FP64 residual stencil                                     */
+#define A2D_K_FACEJAC 6    /* first-order face Jacobian blocks                          */
+#define A2D_K_FACTOR 7     /* block-Thomas factorisation                                */
+/* times `reps` back-to-back launches of one kernel on the plan's current data with CUDA
+ * events on `stream`, for every case of the plan; *ms receives the mean per launch.
+ * Overwrites scratch vectors only (not U). Synchronises. */
+int a2d_time_kernel(a2d_plan* plan, int which, int reps, float* ms, void* stream);
+
 /* ---- explicit RK4 + implicit residual smoothing (aero2d/euler.py:334-346) ---- */
 /* n RK iterations of every case, each followed by circ := Cl M / 2 (euler.py:398-404);
  * res: device [ncases], the RK residual of the last iteration */
