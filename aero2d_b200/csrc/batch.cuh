@@ -21,7 +21,7 @@ namespace a2d {
 constexpr int kTI = 32;        // stencil tile width  (i, circumferential cells)
 constexpr int kTJ = 8;         // stencil tile height (j, wall-normal cells)
 constexpr int kLanes = 32;     // j-lines per line group
-constexpr int kChunk = 2048;   // vector entries per reduction chunk
+constexpr int kChunk = 4096;   // vector entries per reduction chunk (16 per thread of a 256-thread CTA)
 constexpr int kMaxRestart = 64;
 
 // status word bits per case

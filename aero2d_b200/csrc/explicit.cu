@@ -18,7 +18,7 @@ namespace a2d {
 __global__ void __launch_bounds__(256) k_local_dt(Batch b, const double* __restrict__ U, double* __restrict__ dt,
                                                   double cfl) {
   const Tile t = b.tiles[blockIdx.x];
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   const int ni = g.ni, nc = g.nc;
   const size_t N = (size_t)ni * nc, NJ = (size_t)(nc + 1) * ni;
@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(256) k_irs_i(Batch b, const double* __restrict
                                                double e) {
   const int row = blockIdx.x;   // rows enumerated as (case, k, j) via the row table below
   const int cs_id = blockIdx.y;
-  const CaseDev& cs = b.cases[cs_id];
+  const CaseDev cs = b.cases[cs_id];
   const GridDev& g = cs.g;
   const int ni = g.ni, nc = g.nc;
   if (row >= 4 * nc) return;
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(256) k_irs_i(Batch b, const double* __restrict
 // The elimination coefficients depend on j only and are formed once per block.
 __global__ void __launch_bounds__(128) k_irs_j(Batch b, double* __restrict__ R, double e) {
   const int cs_id = blockIdx.y;
-  const CaseDev& cs = b.cases[cs_id];
+  const CaseDev cs = b.cases[cs_id];
   const GridDev& g = cs.g;
   const int ni = g.ni, nc = g.nc;
   extern __shared__ double cpj[];   // nc
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256) k_rk_stage(Batch b, const double* __restr
                                                   const double* __restrict__ R, const double* __restrict__ dt,
                                                   double* __restrict__ U, double a) {
   const Tile t = b.tiles[blockIdx.x];
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   const size_t base = 4 * cs.cell_off;
   for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(256) k_rk_res(Batch b, const double* __restric
                                                 const double* __restrict__ U, const double* __restrict__ dt,
                                                 double* __restrict__ tpart) {
   const Tile t = b.tiles[blockIdx.x];
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   const size_t base = 4 * cs.cell_off;
   double s = 0.0;
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256) k_rk_res(Batch b, const double* __restric
 __global__ void k_rk_finish(Batch b, const double* tpart, const double* coef, double* res, double* circ) {
   const int cs = blockIdx.x * blockDim.x + threadIdx.x;
   if (cs >= b.ncases) return;
-  const CaseDev& c = b.cases[cs];
+  const CaseDev c = b.cases[cs];
   double s = 0.0;
   for (int q = 0; q < c.ntiles; ++q) s += tpart[(size_t)(c.tile0 + q) * kTilePartStride + 3];
   const double N = (double)c.g.ni * (double)c.g.nc;

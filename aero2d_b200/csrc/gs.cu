@@ -1,0 +1,420 @@
+// Arnoldi orthogonalisation of the GMRES cycle: classical Gram-Schmidt run
+// twice (the scheme of aero2d/krylov.py:45-50), in three passes over the
+// Krylov basis per Arnoldi step.
+//
+//   pass 1  k_gs_dots     raw projections V_raw[q] . w and w . w, per chunk
+//   reduce  k_gs_reduce   per case, fixed chunk order: h1_q = s_q (V_raw[q] . w)
+//   pass 2  k_gs_project  w' = w - sum_q V_raw[q] s_q h1_q and V_raw[q] . w' from one
+//                         read of the basis (the entry's basis values stay in
+//                         registers between the subtraction and the projection)
+//   reduce  k_gs_reduce   h2_q
+//   pass 3  k_gs_sub      w'' = w - sum_q V_raw[q] s_q (h1_q + h2_q), written as the
+//                         next raw basis vector, with its squared norm
+//   close   k_gs_close    per case: h_{k+1,k} = ||w''||, the breakdown test against
+//                         eps ||w|| (jax.scipy.sparse.linalg.gmres semantics), the
+//                         Hessenberg column and s_{k+1} = 1 / ||w''||
+//
+// Each thread handles kGE entries of a 4096-entry chunk against up to 32 basis
+// vectors held in registers (the count is a template tier NQ of 8, 16, 24 or
+// 32), so a chunk needs a single block reduction.  Bases of more than 32
+// vectors are processed in slices of 32 by chained launches.  Basis vectors
+// are stored unnormalised with their scale s_q, so no normalisation pass is
+// needed; w' is never stored, since pass 3 subtracts h1 + h2 from the
+// original w (equal to the two successive subtractions in exact arithmetic).
+#include <cfloat>
+#include <type_traits>
+
+#include "batch.cuh"
+#include "gs.cuh"
+
+namespace a2d {
+
+constexpr int kGB = 256;                 // threads per block
+constexpr int kGE = kChunk / kGB;        // entries per thread
+static_assert(kGE * kGB == kChunk, "chunk must split evenly over the block");
+
+// fixed-order reduction of NV values over the block; thread t < NV receives value t
+template <int NV>
+__device__ __forceinline__ double gs_reduce_to_thread(double (&v)[NV], double* scratch /* 8*NV */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) scratch[warp * NV + q] = v[q];
+  }
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < NV) {
+    for (int w = 0; w < kGB / 32; ++w) s += scratch[w * NV + threadIdx.x];
+  }
+  return s;
+}
+
+// s_q (h1_q [+ h2_q]) of the slice's vectors into shared memory
+template <typename TB>
+__device__ __forceinline__ void coef_to_smem(const GsArgs<TB>& a, int cs, int ncases, double* coef, bool both) {
+  for (int q = threadIdx.x; q < a.nq; q += blockDim.x) {
+    const int qq = a.q0 + q;
+    double h = a.h1[(size_t)cs * kHStride + qq];
+    if (both) h += a.h2[(size_t)cs * kHStride + qq];
+    coef[q] = h * a.scale[(size_t)qq * ncases + cs];
+  }
+  __syncthreads();
+}
+
+// vector loads and stores of N consecutive entries (chunks start on multiples of
+// 4 entries and every case vector and basis vector on a 256-byte boundary)
+__device__ __forceinline__ void ldv(const float* p, double (&v)[4]) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ldv(const double* p, double (&v)[4]) {
+  const double2 t0 = *reinterpret_cast<const double2*>(p);
+  const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
+}
+__device__ __forceinline__ void ldv(const float* p, double (&v)[2]) {
+  const float2 t = *reinterpret_cast<const float2*>(p);
+  v[0] = t.x; v[1] = t.y;
+}
+__device__ __forceinline__ void ldv(const double* p, double (&v)[2]) {
+  const double2 t = *reinterpret_cast<const double2*>(p);
+  v[0] = t.x; v[1] = t.y;
+}
+__device__ __forceinline__ void stv(float* p, const double (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+}
+__device__ __forceinline__ void stv(double* p, const double (&v)[4]) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+
+// pass 1 (and the re-projection of the chained path) ---------------------------
+template <typename TB, int NQ>
+__global__ void __launch_bounds__(kGB) k_gs_dots(Batch b, GsArgs<TB> a) {
+  const Chunk ch = b.chunks[blockIdx.x];
+  if (!case_live(b, ch.cs, a.need)) return;
+  const CaseDev cs = b.cases[ch.cs];
+  const size_t base = 4 * cs.cell_off + ch.begin;
+  __shared__ double scratch[8 * (NQ + 1)];
+  const TB* V = a.V + (size_t)a.q0 * a.vstride + base;
+  double acc[NQ + 1];
+#pragma unroll
+  for (int q = 0; q <= NQ; ++q) acc[q] = 0.0;
+#pragma unroll
+  for (int s = 0; s < kGE / 4; ++s) {
+    const int e = 4 * (threadIdx.x + s * kGB);
+    if (e < ch.len) {
+      double w[4];
+      ldv(a.w + base + e, w);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        if (q < a.nq) {
+          double v[4];
+          ldv(V + (size_t)q * a.vstride + e, v);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) acc[q] += v[u] * w[u];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[NQ] += w[u] * w[u];
+    }
+  }
+  const double r = gs_reduce_to_thread<NQ + 1>(acc, scratch);
+  double* part = a.part + (size_t)blockIdx.x * a.pstride;
+  if (threadIdx.x < a.nq) part[a.q0 + threadIdx.x] = r;
+  if (a.with_norm && threadIdx.x == NQ) part[a.norm_slot] = r;
+}
+
+// pass 2, fused: w' = w - V (s h1), then V . w' --------------------------------
+template <typename TB, int NQ>
+__global__ void __launch_bounds__(kGB, 2) k_gs_project(Batch b, GsArgs<TB> a) {
+  const Chunk ch = b.chunks[blockIdx.x];
+  if (!case_live(b, ch.cs, a.need)) return;
+  const CaseDev cs = b.cases[ch.cs];
+  const size_t base = 4 * cs.cell_off + ch.begin;
+  __shared__ double coef[NQ];
+  __shared__ double scratch[8 * NQ];
+  // per-thread slots for the basis entries used twice: [q][thread] pairs in
+  // storage precision (written and read back by the same thread only)
+  extern __shared__ unsigned char gs_dyn[];
+  using Pair = typename std::conditional<sizeof(TB) == 4, float2, double2>::type;
+  Pair* keep = reinterpret_cast<Pair*>(gs_dyn);
+  coef_to_smem(a, ch.cs, b.ncases, coef, false);
+  const TB* V = a.V + base;
+  double acc[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+#pragma unroll 1
+  for (int s = 0; s < kGE / 2; ++s) {
+    const int e = 2 * (threadIdx.x + s * kGB);
+    if (e < ch.len) {
+      double sub0 = 0.0, sub1 = 0.0;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        if (q < a.nq) {
+          const Pair p = *reinterpret_cast<const Pair*>(V + (size_t)q * a.vstride + e);
+          keep[q * kGB + threadIdx.x] = p;
+          sub0 += (double)p.x * coef[q];
+          sub1 += (double)p.y * coef[q];
+        }
+      }
+      double w[2];
+      ldv(a.w + base + e, w);
+      const double wp0 = w[0] - sub0, wp1 = w[1] - sub1;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        if (q < a.nq) {
+          const Pair p = keep[q * kGB + threadIdx.x];
+          acc[q] += (double)p.x * wp0 + (double)p.y * wp1;
+        }
+      }
+    }
+  }
+  const double r = gs_reduce_to_thread<NQ>(acc, scratch);
+  if (threadIdx.x < a.nq) a.part[(size_t)blockIdx.x * a.pstride + threadIdx.x] = r;
+}
+
+// out = in - V (s h): pass 3, and the subtraction slices of the chained path ----
+template <typename TB, int NQ>
+__global__ void __launch_bounds__(kGB) k_gs_sub(Batch b, GsArgs<TB> a) {
+  const Chunk ch = b.chunks[blockIdx.x];
+  if (!case_live(b, ch.cs, a.need)) return;
+  const CaseDev cs = b.cases[ch.cs];
+  const size_t base = 4 * cs.cell_off + ch.begin;
+  __shared__ double coef[NQ];
+  __shared__ double scratch[8];
+  coef_to_smem(a, ch.cs, b.ncases, coef, a.both != 0);
+  const TB* V = a.V + (size_t)a.q0 * a.vstride + base;
+  double nrm = 0.0;
+#pragma unroll
+  for (int s = 0; s < kGE / 4; ++s) {
+    const int e = 4 * (threadIdx.x + s * kGB);
+    if (e < ch.len) {
+      double sub[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        if (q < a.nq) {
+          double v[4];
+          ldv(V + (size_t)q * a.vstride + e, v);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) sub[u] += v[u] * coef[q];
+        }
+      }
+      double w[4];
+      ldv(a.w + base + e, w);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        w[u] = w[u] - sub[u];
+        nrm += w[u] * w[u];
+      }
+      if (a.wout != nullptr) stv(a.wout + base + e, w);
+      if (a.Vout != nullptr) stv(a.Vout + base + e, w);
+    }
+  }
+  if (a.part_norm != nullptr) {
+    double v[1] = {nrm};
+    const double r = gs_reduce_to_thread<1>(v, scratch);
+    if (threadIdx.x == 0) a.part_norm[blockIdx.x] = r;
+  }
+}
+
+// start vector: V_raw[0] = r and its squared norm ------------------------------
+template <typename TB>
+__global__ void __launch_bounds__(kGB) k_gs_start(Batch b, GsArgs<TB> a) {
+  const Chunk ch = b.chunks[blockIdx.x];
+  if (!case_live(b, ch.cs, a.need)) return;
+  const CaseDev cs = b.cases[ch.cs];
+  const size_t base = 4 * cs.cell_off + ch.begin;
+  __shared__ double scratch[8];
+  double nrm = 0.0;
+#pragma unroll
+  for (int s = 0; s < kGE / 4; ++s) {
+    const int e = 4 * (threadIdx.x + s * kGB);
+    if (e < ch.len) {
+      double x[4];
+      ldv(a.w + base + e, x);
+      stv(a.Vout + base + e, x);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) nrm += x[u] * x[u];
+    }
+  }
+  double v[1] = {nrm};
+  const double r = gs_reduce_to_thread<1>(v, scratch);
+  if (threadIdx.x == 0) a.part_norm[blockIdx.x] = r;
+}
+
+// per-case reduction of the chunk partials, one block per case ----------------
+__global__ void k_gs_reduce(Batch b, GsReduceArgs a) {
+  const int cs_id = blockIdx.x;
+  if (!case_live(b, cs_id, a.need)) return;
+  const CaseDev cs = b.cases[cs_id];
+  const int nred = a.nq + (a.wn0 != nullptr ? 1 : 0);
+  for (int q = threadIdx.x; q < nred; q += blockDim.x) {
+    double s = 0.0;
+    for (int c = 0; c < cs.nchunks; ++c) s += a.part[(size_t)(cs.chunk0 + c) * a.pstride + q];
+    if (q < a.nq) a.h[(size_t)cs_id * kHStride + q] = s * a.scale[(size_t)q * b.ncases + cs_id];
+    else a.wn0[cs_id] = sqrt(s);
+  }
+}
+
+// per-case close of an Arnoldi step (k >= 0) or of the start vector (k = -1) ----
+__global__ void k_gs_close(Batch b, GsCloseArgs a) {
+  const int cs_id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cs_id >= b.ncases) return;
+  if ((a.live[cs_id] & a.need) != a.need) return;
+  const CaseDev cs = b.cases[cs_id];
+  double s = 0.0;
+  for (int c = 0; c < cs.nchunks; ++c) s += a.part_norm[cs.chunk0 + c];
+  const double hn = sqrt(s);
+  CaseCtl& c = a.ctl[cs_id];
+  if (a.k < 0) {
+    // _safe_normalize of the preconditioned residual: threshold eps
+    const bool use = hn > DBL_EPSILON;
+    const double beta = use ? hn : 0.0;
+    a.scale[cs_id] = use ? 1.0 / hn : 0.0;
+    c.beta = beta;
+    c.k_used = 0;
+    const bool run = beta > c.ptol && c.bnorm > 0.0;
+    if (run) a.live[cs_id] |= kLiveKrylov;
+    else a.live[cs_id] &= ~kLiveKrylov;
+    return;
+  }
+  const int k = a.k;
+  const bool use = hn > DBL_EPSILON * a.wn0[cs_id];
+  double* H = a.H + (size_t)cs_id * kMaxRestart * (kMaxRestart + 1) + (size_t)k * (kMaxRestart + 1);
+  const double* h1 = a.h1 + (size_t)cs_id * kHStride;
+  const double* h2 = a.h2 + (size_t)cs_id * kHStride;
+  for (int q = 0; q <= k; ++q) H[q] = h1[q] + h2[q];
+  H[k + 1] = use ? hn : 0.0;
+  a.scale[(size_t)(k + 1) * b.ncases + cs_id] = use ? 1.0 / hn : 0.0;
+  c.k_used = k + 1;
+  if (!use) a.live[cs_id] &= ~kLiveKrylov;
+}
+
+// ---------------------------------------------------------------------------
+// host side: tier dispatch and the chained path for more than 32 vectors
+// ---------------------------------------------------------------------------
+constexpr int kSlice = 32;
+
+// dynamic shared memory of pass 2 for a tier: one entry pair per vector and thread
+template <typename TB, int NQ>
+constexpr size_t project_smem() {
+  return (size_t)NQ * kGB * 2 * sizeof(TB);
+}
+
+#define A2D_GS_DISPATCH(KERNEL, SMEM)                                                      \
+  template <typename TB>                                                                   \
+  static void dispatch_##KERNEL(const Batch& b, const GsArgs<TB>& a, cudaStream_t s) {     \
+    if (!b.nchunks) return;                                                                \
+    if (a.nq <= 8) KERNEL<TB, 8><<<b.nchunks, kGB, SMEM(8), s>>>(b, a);                     \
+    else if (a.nq <= 16) KERNEL<TB, 16><<<b.nchunks, kGB, SMEM(16), s>>>(b, a);             \
+    else if (a.nq <= 24) KERNEL<TB, 24><<<b.nchunks, kGB, SMEM(24), s>>>(b, a);             \
+    else KERNEL<TB, 32><<<b.nchunks, kGB, SMEM(32), s>>>(b, a);                             \
+  }
+#define A2D_NO_SMEM(N) 0
+#define A2D_PROJECT_SMEM(N) project_smem<TB, N>()
+A2D_GS_DISPATCH(k_gs_dots, A2D_NO_SMEM)
+A2D_GS_DISPATCH(k_gs_project, A2D_PROJECT_SMEM)
+A2D_GS_DISPATCH(k_gs_sub, A2D_NO_SMEM)
+#undef A2D_GS_DISPATCH
+#undef A2D_NO_SMEM
+#undef A2D_PROJECT_SMEM
+
+// allows the pass-2 tiers their dynamic shared memory (once per process and type)
+template <typename TB>
+cudaError_t gs_configure() {
+  cudaError_t e = cudaSuccess;
+  cudaError_t r;
+  if ((r = cudaFuncSetAttribute(k_gs_project<TB, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)project_smem<TB, 8>())) != cudaSuccess) e = r;
+  if ((r = cudaFuncSetAttribute(k_gs_project<TB, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)project_smem<TB, 16>())) != cudaSuccess) e = r;
+  if ((r = cudaFuncSetAttribute(k_gs_project<TB, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)project_smem<TB, 24>())) != cudaSuccess) e = r;
+  if ((r = cudaFuncSetAttribute(k_gs_project<TB, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)project_smem<TB, 32>())) != cudaSuccess) e = r;
+  return e;
+}
+template cudaError_t gs_configure<double>();
+template cudaError_t gs_configure<float>();
+
+template <typename TB>
+void launch_gs_dots(const Batch& b, const GsArgs<TB>& a0, cudaStream_t s) {
+  GsArgs<TB> a = a0;
+  a.norm_slot = a0.nq;
+  for (int q0 = 0; q0 < a0.nq; q0 += kSlice) {
+    a.q0 = q0;
+    a.nq = a0.nq - q0 < kSlice ? a0.nq - q0 : kSlice;
+    a.with_norm = a0.with_norm && q0 == 0;
+    dispatch_k_gs_dots<TB>(b, a, s);
+  }
+}
+
+template <typename TB>
+void launch_gs_project(const Batch& b, const GsArgs<TB>& a0, cudaStream_t s) {
+  if (a0.nq <= kSlice) {
+    GsArgs<TB> a = a0;
+    a.q0 = 0;
+    dispatch_k_gs_project<TB>(b, a, s);
+    return;
+  }
+  // chained: w' = w - V (s h1) into the scratch vector, then its projections
+  GsArgs<TB> a = a0;
+  a.both = 0;
+  a.Vout = nullptr;
+  a.part_norm = nullptr;
+  for (int q0 = 0; q0 < a0.nq; q0 += kSlice) {
+    a.q0 = q0;
+    a.nq = a0.nq - q0 < kSlice ? a0.nq - q0 : kSlice;
+    a.w = q0 == 0 ? a0.w : a0.tmp;
+    a.wout = a0.tmp;
+    dispatch_k_gs_sub<TB>(b, a, s);
+  }
+  GsArgs<TB> d = a0;
+  d.w = a0.tmp;
+  d.with_norm = 0;
+  launch_gs_dots<TB>(b, d, s);
+}
+
+template <typename TB>
+void launch_gs_finish(const Batch& b, const GsArgs<TB>& a0, cudaStream_t s) {
+  GsArgs<TB> a = a0;
+  a.both = 1;
+  for (int q0 = 0; q0 < a0.nq; q0 += kSlice) {
+    const bool last = q0 + kSlice >= a0.nq;
+    a.q0 = q0;
+    a.nq = a0.nq - q0 < kSlice ? a0.nq - q0 : kSlice;
+    a.w = q0 == 0 ? a0.w : a0.tmp;
+    a.wout = last ? nullptr : a0.tmp;
+    a.Vout = last ? a0.Vout : nullptr;
+    a.part_norm = last ? a0.part_norm : nullptr;
+    dispatch_k_gs_sub<TB>(b, a, s);
+  }
+}
+
+template <typename TB>
+void launch_gs_start(const Batch& b, const GsArgs<TB>& a, cudaStream_t s) {
+  if (b.nchunks) k_gs_start<TB><<<b.nchunks, kGB, 0, s>>>(b, a);
+}
+void launch_gs_reduce(const Batch& b, const GsReduceArgs& a, cudaStream_t s) {
+  if (b.ncases) k_gs_reduce<<<b.ncases, 64, 0, s>>>(b, a);
+}
+void launch_gs_close(const Batch& b, const GsCloseArgs& a, cudaStream_t s) {
+  k_gs_close<<<(b.ncases + 63) / 64, 64, 0, s>>>(b, a);
+}
+
+#define A2D_GS_INST(TB)                                                                 \
+  template void launch_gs_dots<TB>(const Batch&, const GsArgs<TB>&, cudaStream_t);     \
+  template void launch_gs_project<TB>(const Batch&, const GsArgs<TB>&, cudaStream_t);  \
+  template void launch_gs_finish<TB>(const Batch&, const GsArgs<TB>&, cudaStream_t);   \
+  template void launch_gs_start<TB>(const Batch&, const GsArgs<TB>&, cudaStream_t);
+A2D_GS_INST(double)
+A2D_GS_INST(float)
+#undef A2D_GS_INST
+
+}  // namespace a2d

@@ -11,6 +11,7 @@ template <typename VT>
 struct StencilArgs {
   const double* U = nullptr;       // conserved state (FP64), packed cell vectors
   const VT* V = nullptr;           // tangent direction (linearised mode)
+  const double* vscale = nullptr;  // per-case factor applied to V (a raw Krylov vector's 1/norm)
   const double* circ_in = nullptr; // per-case circulation; nullptr: Gamma(U) from the wall rows
   const double* diag = nullptr;    // per-cell vol / dtau (linearised mode; nullptr: J v alone)
   const double* bvec = nullptr;    // linearised mode: out = b - (diag v + J v) when set

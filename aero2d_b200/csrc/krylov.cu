@@ -63,145 +63,6 @@ constexpr int kVB = 256;                 // threads per vector block
 constexpr int kPer = kChunk / kVB;       // entries per thread
 
 // ---------------------------------------------------------------------------
-// partial dot products of w with V[0..nq) (and optionally w.w), per chunk
-// ---------------------------------------------------------------------------
-template <typename TB>
-__global__ void __launch_bounds__(kVB) k_dots(Batch b, DotArgs<TB> a) {
-  const Chunk ch = b.chunks[blockIdx.x];
-  if (!case_live(b, ch.cs, a.need)) return;
-  const CaseDev& cs = b.cases[ch.cs];
-  const size_t base = 4 * cs.cell_off + ch.begin;
-  __shared__ double scratch[32 * 8];
-  double wv[kPer];
-#pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int e = threadIdx.x + s * kVB;
-    wv[s] = e < ch.len ? a.w[base + e] : 0.0;
-  }
-  for (int q0 = 0; q0 < a.nq; q0 += 8) {
-    double acc[8];
-#pragma unroll
-    for (int qq = 0; qq < 8; ++qq) {
-      acc[qq] = 0.0;
-      const int q = q0 + qq;
-      if (q < a.nq) {
-        const TB* v = a.V + (size_t)q * a.vstride + base;
-#pragma unroll
-        for (int s = 0; s < kPer; ++s) {
-          const int e = threadIdx.x + s * kVB;
-          if (e < ch.len) acc[qq] += (double)v[e] * wv[s];
-        }
-      }
-    }
-    block_sum_k<double, 8>(acc, scratch);
-    if (threadIdx.x == 0) {
-#pragma unroll
-      for (int qq = 0; qq < 8; ++qq)
-        if (q0 + qq < a.nq) a.part[(size_t)blockIdx.x * a.pstride + q0 + qq] = acc[qq];
-    }
-  }
-  if (a.with_norm) {
-    double acc[1] = {0.0};
-#pragma unroll
-    for (int s = 0; s < kPer; ++s) acc[0] += wv[s] * wv[s];
-    block_sum_k<double, 1>(acc, scratch);
-    if (threadIdx.x == 0) a.part[(size_t)blockIdx.x * a.pstride + a.nq] = acc[0];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// w <- w - V h, h reduced from the chunk partials of the case; optional
-// partial norm of the new w
-// ---------------------------------------------------------------------------
-template <typename TB>
-__global__ void __launch_bounds__(kVB) k_update(Batch b, UpdateArgs<TB> a) {
-  const Chunk ch = b.chunks[blockIdx.x];
-  if (!case_live(b, ch.cs, a.need)) return;
-  const CaseDev& cs = b.cases[ch.cs];
-  const size_t base = 4 * cs.cell_off + ch.begin;
-  __shared__ double sh[kMaxRestart + 2];
-  __shared__ double scratch[32];
-  const int nred = a.nq + (a.wn0 != nullptr ? 1 : 0);
-  for (int q = threadIdx.x; q < nred; q += blockDim.x) {
-    double s = 0.0;
-    for (int c = 0; c < cs.nchunks; ++c) s += a.part[(size_t)(cs.chunk0 + c) * a.pstride + q];
-    sh[q] = s;
-  }
-  __syncthreads();
-  if (blockIdx.x == cs.chunk0 && threadIdx.x == 0) {
-    for (int q = 0; q < a.nq; ++q) a.hstore[(size_t)ch.cs * (kMaxRestart + 1) + q] = sh[q];
-    if (a.wn0 != nullptr) a.wn0[ch.cs] = sqrt(sh[a.nq]);
-  }
-  double nrm = 0.0;
-#pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int e = threadIdx.x + s * kVB;
-    if (e < ch.len) {
-      double acc = 0.0;
-      for (int q = 0; q < a.nq; ++q) acc += (double)a.V[(size_t)q * a.vstride + base + e] * sh[q];
-      const double wn = a.w[base + e] - acc;
-      a.w[base + e] = wn;
-      nrm += wn * wn;
-    }
-  }
-  if (a.part_norm != nullptr) {
-    double v[1] = {nrm};
-    block_sum_k<double, 1>(v, scratch);
-    if (threadIdx.x == 0) a.part_norm[blockIdx.x] = v[0];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Arnoldi closing step: hn = ||w||, breakdown test against eps * ||w_before||,
-// V[k+1] = w / hn, Hessenberg column k = h1 + h2 and hn
-// ---------------------------------------------------------------------------
-template <typename TB>
-__global__ void __launch_bounds__(kVB) k_normalize(Batch b, NormalizeArgs<TB> a) {
-  const Chunk ch = b.chunks[blockIdx.x];
-  if (!case_live(b, ch.cs, a.need)) return;
-  const CaseDev& cs = b.cases[ch.cs];
-  const size_t base = 4 * cs.cell_off + ch.begin;
-  double s = 0.0;
-  for (int c = 0; c < cs.nchunks; ++c) s += a.part_norm[cs.chunk0 + c];
-  const double hn = sqrt(s);
-  double thresh;
-  if (a.k < 0) {
-    thresh = DBL_EPSILON;                 // start vector: _safe_normalize default threshold
-  } else {
-    thresh = DBL_EPSILON * a.wn0[ch.cs];  // Arnoldi vector: eps * norm before orthogonalisation
-  }
-  const bool use = hn > thresh;
-  const double inv = use ? 1.0 / hn : 0.0;
-#pragma unroll
-  for (int q = 0; q < kPer; ++q) {
-    const int e = threadIdx.x + q * kVB;
-    if (e < ch.len) a.Vout[base + e] = use ? TB(a.w[base + e] / hn) : TB(0);
-  }
-  (void)inv;
-  if (blockIdx.x == cs.chunk0 && threadIdx.x == 0) {
-    CaseCtl& c = a.ctl[ch.cs];
-    if (a.k < 0) {
-      const double beta = use ? hn : 0.0;
-      c.beta = beta;
-      c.k_used = 0;
-      // one GMRES cycle runs only if the preconditioned residual exceeds ptol
-      const bool run = beta > c.ptol && c.bnorm > 0.0;
-      if (!run) a.live[ch.cs] &= ~kLiveKrylov;
-      else a.live[ch.cs] |= kLiveKrylov;
-    } else {
-      const int k = a.k;
-      double* H = a.H + (size_t)ch.cs * kMaxRestart * (kMaxRestart + 1) + (size_t)k * (kMaxRestart + 1);
-      const double* h1 = a.h1 + (size_t)ch.cs * (kMaxRestart + 1);
-      const double* h2 = a.h2 + (size_t)ch.cs * (kMaxRestart + 1);
-      for (int q = 0; q <= k; ++q) H[q] = h1[q] + h2[q];
-      H[k + 1] = use ? hn : 0.0;
-      c.k_used = k + 1;
-      if (!use) a.live[ch.cs] &= ~kLiveKrylov;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Hessenberg least squares min || beta e1 - H y || by Givens rotations, one
 // thread per case (H column k = Arnoldi step k)
 // ---------------------------------------------------------------------------
@@ -255,16 +116,20 @@ template <typename TB>
 __global__ void __launch_bounds__(kVB) k_combine(Batch b, CombineArgs<TB> a) {
   const Chunk ch = b.chunks[blockIdx.x];
   if (!case_live(b, ch.cs, a.need)) return;
-  const CaseDev& cs = b.cases[ch.cs];
+  const CaseDev cs = b.cases[ch.cs];
   const size_t base = 4 * cs.cell_off + ch.begin;
   const int k = a.ctl[ch.cs].k_used;
   const double* y = a.y + (size_t)ch.cs * kMaxRestart;
+  __shared__ double ys[kMaxRestart];
+  // raw basis vectors carry their normalisation in scale[q][case]
+  for (int q = threadIdx.x; q < k; q += blockDim.x) ys[q] = y[q] * a.scale[(size_t)q * b.ncases + ch.cs];
+  __syncthreads();
 #pragma unroll
   for (int s = 0; s < kPer; ++s) {
     const int e = threadIdx.x + s * kVB;
     if (e < ch.len) {
       double acc = 0.0;
-      for (int q = 0; q < k; ++q) acc += (double)a.V[(size_t)q * a.vstride + base + e] * y[q];
+      for (int q = 0; q < k; ++q) acc += (double)a.V[(size_t)q * a.vstride + base + e] * ys[q];
       a.out[base + e] = a.x0[base + e] + acc;
     }
   }
@@ -275,7 +140,7 @@ __global__ void k_gm_setup(Batch b, const double* part, int pstride, CaseCtl* ct
   const int cs = blockIdx.x * blockDim.x + threadIdx.x;
   if (cs >= b.ncases) return;
   if (!case_live(b, cs, kLiveNewton)) return;
-  const CaseDev& c = b.cases[cs];
+  const CaseDev c = b.cases[cs];
   double sb = 0.0, sx = 0.0;
   for (int q = 0; q < c.nchunks; ++q) {
     sb += part[(size_t)(c.chunk0 + q) * pstride + 0];
@@ -293,7 +158,7 @@ __global__ void __launch_bounds__(kVB) k_norms2(Batch b, const double* x, const 
                                                 int pstride, uint32_t need) {
   const Chunk ch = b.chunks[blockIdx.x];
   if (!case_live(b, ch.cs, need)) return;
-  const CaseDev& cs = b.cases[ch.cs];
+  const CaseDev cs = b.cases[ch.cs];
   const size_t base = 4 * cs.cell_off + ch.begin;
   __shared__ double scratch[64];
   double acc[2] = {0.0, 0.0};
@@ -313,7 +178,7 @@ __global__ void __launch_bounds__(kVB) k_norms2(Batch b, const double* x, const 
 __global__ void __launch_bounds__(kVB) k_norm1(Batch b, const double* x, double* part, uint32_t need) {
   const Chunk ch = b.chunks[blockIdx.x];
   if (!case_live(b, ch.cs, need)) return;
-  const CaseDev& cs = b.cases[ch.cs];
+  const CaseDev cs = b.cases[ch.cs];
   const size_t base = 4 * cs.cell_off + ch.begin;
   __shared__ double scratch[32];
   double acc[1] = {0.0};
@@ -330,7 +195,7 @@ __global__ void __launch_bounds__(256) k_update_rel(Batch b, const double* U, co
                                                     double* tpart, uint32_t need) {
   const Tile t = b.tiles[blockIdx.x];
   if (!case_live(b, t.cs, need)) return;
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   const size_t base = 4 * cs.cell_off;
   double m = 0.0;
@@ -358,7 +223,7 @@ __global__ void __launch_bounds__(256) k_update_check(Batch b, const double* U, 
                                                       uint32_t need) {
   const Tile t = b.tiles[blockIdx.x];
   if (!case_live(b, t.cs, need)) return;
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   double rel = 0.0;
   for (int q = 0; q < cs.ntiles; ++q) {
@@ -392,7 +257,7 @@ __global__ void k_controller(Batch b, const double* tpart, CaseCtl* ctl, uint32_
   const int cs = blockIdx.x * blockDim.x + threadIdx.x;
   if (cs >= b.ncases) return;
   if (!(live[cs] & kLiveNewton)) return;
-  const CaseDev& c = b.cases[cs];
+  const CaseDev c = b.cases[cs];
   CaseCtl& s = ctl[cs];
   double sr = 0.0, nbad = 0.0;
   for (int q = 0; q < c.ntiles; ++q) {
@@ -428,7 +293,7 @@ __global__ void __launch_bounds__(256) k_commit(Batch b, double* U, const double
   const Tile t = b.tiles[blockIdx.x];
   const CaseCtl& s = ctl[t.cs];
   if (!s.commit || !s.stepped) return;
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   const size_t base = 4 * cs.cell_off;
   const double omega = s.omega;
@@ -452,19 +317,6 @@ __global__ void k_mark_stepped(int ncases, const uint32_t* live, CaseCtl* ctl) {
 
 // ---------------------------------------------------------------------------
 // launchers
-// ---------------------------------------------------------------------------
-template <typename TB>
-void launch_dots(const Batch& b, const DotArgs<TB>& a, cudaStream_t s) {
-  if (b.nchunks) k_dots<TB><<<b.nchunks, kVB, 0, s>>>(b, a);
-}
-template <typename TB>
-void launch_update(const Batch& b, const UpdateArgs<TB>& a, cudaStream_t s) {
-  if (b.nchunks) k_update<TB><<<b.nchunks, kVB, 0, s>>>(b, a);
-}
-template <typename TB>
-void launch_normalize(const Batch& b, const NormalizeArgs<TB>& a, cudaStream_t s) {
-  if (b.nchunks) k_normalize<TB><<<b.nchunks, kVB, 0, s>>>(b, a);
-}
 template <typename TB>
 void launch_combine(const Batch& b, const CombineArgs<TB>& a, cudaStream_t s) {
   if (b.nchunks) k_combine<TB><<<b.nchunks, kVB, 0, s>>>(b, a);
@@ -503,12 +355,6 @@ void launch_mark_stepped(const Batch& b, const uint32_t* live, CaseCtl* ctl, cud
   k_mark_stepped<<<(b.ncases + 63) / 64, 64, 0, s>>>(b.ncases, live, ctl);
 }
 
-template void launch_dots<double>(const Batch&, const DotArgs<double>&, cudaStream_t);
-template void launch_dots<float>(const Batch&, const DotArgs<float>&, cudaStream_t);
-template void launch_update<double>(const Batch&, const UpdateArgs<double>&, cudaStream_t);
-template void launch_update<float>(const Batch&, const UpdateArgs<float>&, cudaStream_t);
-template void launch_normalize<double>(const Batch&, const NormalizeArgs<double>&, cudaStream_t);
-template void launch_normalize<float>(const Batch&, const NormalizeArgs<float>&, cudaStream_t);
 template void launch_combine<double>(const Batch&, const CombineArgs<double>&, cudaStream_t);
 template void launch_combine<float>(const Batch&, const CombineArgs<float>&, cudaStream_t);
 

@@ -15,60 +15,17 @@ struct CtlParams {
 };
 
 template <typename TB>
-struct DotArgs {
-  const double* w = nullptr;
-  const TB* V = nullptr;
-  size_t vstride = 0;      // entries between consecutive basis vectors
-  int nq = 0;              // number of basis vectors
-  int with_norm = 0;       // also w.w in slot nq
-  double* part = nullptr;  // [chunk][pstride]
-  int pstride = 0;
-  uint32_t need = 0;
-};
-
-template <typename TB>
-struct UpdateArgs {
-  double* w = nullptr;
-  const TB* V = nullptr;
-  size_t vstride = 0;
-  int nq = 0;
-  const double* part = nullptr;  // dot partials to reduce
-  int pstride = 0;
-  double* hstore = nullptr;      // [case][kMaxRestart+1] reduced coefficients
-  double* wn0 = nullptr;         // if set: sqrt of slot nq stored per case (norm before orthogonalisation)
-  double* part_norm = nullptr;   // if set: per-chunk squared norm of the updated w
-  uint32_t need = 0;
-};
-
-template <typename TB>
-struct NormalizeArgs {
-  const double* w = nullptr;
-  TB* Vout = nullptr;
-  const double* part_norm = nullptr;
-  const double* wn0 = nullptr;
-  const double* h1 = nullptr;
-  const double* h2 = nullptr;
-  double* H = nullptr;            // [case][kMaxRestart][kMaxRestart+1], column k = step k
-  CaseCtl* ctl = nullptr;
-  uint32_t* live = nullptr;
-  int k = -1;                     // -1: start vector
-  uint32_t need = 0;
-};
-
-template <typename TB>
 struct CombineArgs {
   const double* x0 = nullptr;
   const TB* V = nullptr;
   size_t vstride = 0;
   const double* y = nullptr;
+  const double* scale = nullptr;  // [q][case] scale of raw basis vector q
   const CaseCtl* ctl = nullptr;
   double* out = nullptr;
   uint32_t need = 0;
 };
 
-template <typename TB> void launch_dots(const Batch& b, const DotArgs<TB>& a, cudaStream_t s);
-template <typename TB> void launch_update(const Batch& b, const UpdateArgs<TB>& a, cudaStream_t s);
-template <typename TB> void launch_normalize(const Batch& b, const NormalizeArgs<TB>& a, cudaStream_t s);
 template <typename TB> void launch_combine(const Batch& b, const CombineArgs<TB>& a, cudaStream_t s);
 void launch_lstsq(const Batch& b, const uint32_t* live, CaseCtl* ctl, double* H, double* y, double* scr,
                   cudaStream_t s);

@@ -86,7 +86,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_face_jac(Batch b, JacArgs a) {
   const Tile t = b.tiles[blockIdx.x];
   if (!case_live(b, t.cs, a.need)) return;
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   Metric<T> m{g};
   const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   const Group grp = b.groups[gid];
   if (!case_live(b, grp.cs, a.need)) return;
   if (lane >= grp.n) return;
-  const CaseDev& cs = b.cases[grp.cs];
+  const CaseDev cs = b.cases[grp.cs];
   const GridDev& g = cs.g;
   const int ni = g.ni, nc = g.nc;
   const int i = grp.i0 + lane;
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(256) k_rhs(Batch b, RhsArgs a) {
   if (!case_live(b, t.cs, a.need)) return;
   const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
   if (lane >= t.ti || row >= t.tj) return;
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   const int ni = g.ni, nc = g.nc;
   const int i = t.i0 + lane, j = t.j0 + row, grp = t.i0 / kLanes;
@@ -378,118 +378,96 @@ __global__ void __launch_bounds__(256) k_rhs(Batch b, RhsArgs a) {
 // the sequential part of the block-Thomas solve, in place on x:
 //   forward   d_j = e_j + G_j d_{j-1}
 //   backward  x_j = d_j - C_j x_{j+1}
-// one thread per line; the operands of the next 4 steps are loaded ahead so
-// each step waits on a quarter of the memory latency
+// Four threads per line, one per row of the 4x4 blocks; the quad exchanges
+// the previous step's 4-vector by shuffles.  Each thread keeps the operands of
+// its row for the next kAhead steps in registers (one FP64 vector entry and
+// four block entries per step), so a step waits on 1/kAhead of the memory
+// latency, and a 32-line group fills four warps.
 // ---------------------------------------------------------------------------
+constexpr int kAhead = 8;
+
 template <typename TF>
-struct StepBuf {
-  double v[4];
-  TF M[16];
+struct RowStep {
+  double v;
+  TF m[4];
 };
 
 template <typename TF>
-__device__ __forceinline__ void load_step(StepBuf<TF>& s, const double* x, const TF* M, const CaseDev& cs,
-                                          const GridDev& g, int grp, int lane, int i, int j) {
+__device__ __forceinline__ void load_row(RowStep<TF>& s, const double* x, const TF* M, const CaseDev& cs,
+                                         const GridDev& g, int grp, int lane, int i, int q, int j) {
   if (j < 0 || j >= g.nc) return;
+  s.v = x[vidx(g, q, j, i)];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) s.v[k] = x[vidx(g, k, j, i)];
-#pragma unroll
-  for (int e = 0; e < 16; ++e) s.M[e] = M[lbidx(cs.rows_nc, g.nc, grp, j, e, lane)];
+  for (int c = 0; c < 4; ++c) s.m[c] = M[lbidx(cs.rows_nc, g.nc, grp, j, q * 4 + c, lane)];
 }
 
-template <typename TF>
-__device__ __forceinline__ void fwd_step(const StepBuf<TF>& s, double d[4], double* x, const GridDev& g, int i,
-                                         int j) {
-  double nd[4];
+// the 4 components of the quad's current vector, from the quad's lanes
+__device__ __forceinline__ void quad_gather(double mine, int base, double out[4]) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    double acc = s.v[q];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc += (double)s.M[q * 4 + k] * d[k];
-    nd[q] = acc;
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    d[q] = nd[q];
-    x[vidx(g, q, j, i)] = nd[q];
-  }
+  for (int c = 0; c < 4; ++c) out[c] = __shfl_sync(0xffffffffu, mine, base | c);
 }
 
-template <typename TF>
-__device__ __forceinline__ void bwd_step(const StepBuf<TF>& s, double xn[4], double* x, const GridDev& g, int i,
-                                         int j) {
-  double nx[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    double acc = 0.0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc += (double)s.M[q * 4 + k] * xn[k];
-    nx[q] = s.v[q] - acc;
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    xn[q] = nx[q];
-    x[vidx(g, q, j, i)] = nx[q];
-  }
-}
-
+// one CTA of 128 threads per 32-line group: warp w holds lines 8w..8w+7,
+// lane 4l+q is row q of line l
 template <typename TF>
 __global__ void __launch_bounds__(128) k_lines(Batch b, LinesArgs a) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gid = blockIdx.x * 4 + warp;
+  const int gid = blockIdx.x;
   if (gid >= b.ngroups) return;
   const Group grp = b.groups[gid];
   if (!case_live(b, grp.cs, a.need)) return;
-  if (lane >= grp.n) return;
-  const CaseDev& cs = b.cases[grp.cs];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int l = warp * 8 + (lane >> 2);       // line within the group
+  const int q = lane & 3;                      // row of the 4x4 blocks owned
+  const int base = lane & ~3;                  // first lane of the quad
+  const bool owner = l < grp.n;                // quads past the group's last line only shuffle
+  const int ll = owner ? l : grp.n - 1;        // their loads stay on a valid line
+  const CaseDev cs = b.cases[grp.cs];
   const GridDev& g = cs.g;
   const int nc = g.nc;
-  const int i = grp.i0 + lane;
+  const int i = grp.i0 + ll;
   double* x = a.x + 4 * cs.cell_off;
   const TF* G = static_cast<const TF*>(a.G);
   const TF* CF = static_cast<const TF*>(a.CF);
-  StepBuf<TF> b0, b1, b2, b3;
-  double d[4] = {0.0, 0.0, 0.0, 0.0};
-  load_step(b0, x, G, cs, g, grp.g, lane, i, 0);
-  load_step(b1, x, G, cs, g, grp.g, lane, i, 1);
-  load_step(b2, x, G, cs, g, grp.g, lane, i, 2);
-  load_step(b3, x, G, cs, g, grp.g, lane, i, 3);
-  for (int j = 0; j < nc; j += 4) {
-    fwd_step(b0, d, x, g, i, j);
-    load_step(b0, x, G, cs, g, grp.g, lane, i, j + 4);
-    if (j + 1 < nc) {
-      fwd_step(b1, d, x, g, i, j + 1);
-      load_step(b1, x, G, cs, g, grp.g, lane, i, j + 5);
-    }
-    if (j + 2 < nc) {
-      fwd_step(b2, d, x, g, i, j + 2);
-      load_step(b2, x, G, cs, g, grp.g, lane, i, j + 6);
-    }
-    if (j + 3 < nc) {
-      fwd_step(b3, d, x, g, i, j + 3);
-      load_step(b3, x, G, cs, g, grp.g, lane, i, j + 7);
+  RowStep<TF> buf[kAhead];
+  // forward: d_j = e_j + G_j d_{j-1}
+  double d = 0.0;
+#pragma unroll
+  for (int u = 0; u < kAhead; ++u) load_row(buf[u], x, G, cs, g, grp.g, ll, i, q, u);
+  for (int j0 = 0; j0 < nc; j0 += kAhead) {
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const int j = j0 + u;
+      if (j < nc) {
+        double dp[4];
+        quad_gather(d, base, dp);
+        double acc = buf[u].v;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc += (double)buf[u].m[c] * dp[c];
+        d = acc;
+        if (owner) x[vidx(g, q, j, i)] = acc;
+        load_row(buf[u], x, G, cs, g, grp.g, ll, i, q, j + kAhead);
+      }
     }
   }
-  double xn[4] = {0.0, 0.0, 0.0, 0.0};
+  // backward: x_j = d_j - C_j x_{j+1}
+  double xn = 0.0;
   const int top = nc - 1;
-  load_step(b0, x, CF, cs, g, grp.g, lane, i, top);
-  load_step(b1, x, CF, cs, g, grp.g, lane, i, top - 1);
-  load_step(b2, x, CF, cs, g, grp.g, lane, i, top - 2);
-  load_step(b3, x, CF, cs, g, grp.g, lane, i, top - 3);
-  for (int j = top; j >= 0; j -= 4) {
-    bwd_step(b0, xn, x, g, i, j);
-    load_step(b0, x, CF, cs, g, grp.g, lane, i, j - 4);
-    if (j - 1 >= 0) {
-      bwd_step(b1, xn, x, g, i, j - 1);
-      load_step(b1, x, CF, cs, g, grp.g, lane, i, j - 5);
-    }
-    if (j - 2 >= 0) {
-      bwd_step(b2, xn, x, g, i, j - 2);
-      load_step(b2, x, CF, cs, g, grp.g, lane, i, j - 6);
-    }
-    if (j - 3 >= 0) {
-      bwd_step(b3, xn, x, g, i, j - 3);
-      load_step(b3, x, CF, cs, g, grp.g, lane, i, j - 7);
+#pragma unroll
+  for (int u = 0; u < kAhead; ++u) load_row(buf[u], x, CF, cs, g, grp.g, ll, i, q, top - u);
+  for (int j0 = top; j0 >= 0; j0 -= kAhead) {
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u) {
+      const int j = j0 - u;
+      if (j >= 0) {
+        double xp[4];
+        quad_gather(xn, base, xp);
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc += (double)buf[u].m[c] * xp[c];
+        xn = buf[u].v - acc;
+        if (owner) x[vidx(g, q, j, i)] = xn;
+        load_row(buf[u], x, CF, cs, g, grp.g, ll, i, q, j - kAhead);
+      }
     }
   }
 }
@@ -512,7 +490,7 @@ void launch_rhs(const Batch& b, const RhsArgs& a, cudaStream_t s) {
 template <typename TF>
 void launch_lines(const Batch& b, const LinesArgs& a, cudaStream_t s) {
   if (b.ngroups == 0) return;
-  k_lines<TF><<<(b.ngroups + 3) / 4, 128, 0, s>>>(b, a);
+  k_lines<TF><<<b.ngroups, 128, 0, s>>>(b, a);
 }
 
 template void launch_face_jac<double>(const Batch&, const JacArgs&, cudaStream_t);

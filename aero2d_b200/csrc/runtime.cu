@@ -14,12 +14,14 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "aero2d_b200.h"
 #include "batch.cuh"
 #include "explicit.cuh"
 #include "kernels.cuh"
+#include "gs.cuh"
 #include "krylov.cuh"
 #include "physics.cuh"
 
@@ -106,7 +108,7 @@ struct a2d_plan {
   size_t o_cases = 0, o_tiles = 0, o_chunks = 0, o_groups = 0, o_cpoff = 0, o_live = 0, o_ctl = 0;
   size_t o_vec[kNumVec] = {};
   size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_G = 0, o_V = 0;
-  size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_y = 0, o_lsq = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
+  size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_lsq = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
   size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0;
   int pstride = 0;
   size_t bytes = 0;
@@ -193,8 +195,9 @@ static void layout(a2d_plan* P) {
   P->o_G = cv.take(P->tj * lb * P->rows_nc);
   P->o_V = cv.take(P->tb * 4 * C * (size_t)(P->m + 1));
   P->o_H = cv.take(8 * (size_t)B * kMaxRestart * (kMaxRestart + 1));
-  P->o_h1 = cv.take(8 * (size_t)B * (kMaxRestart + 1));
-  P->o_h2 = cv.take(8 * (size_t)B * (kMaxRestart + 1));
+  P->o_h1 = cv.take(8 * (size_t)B * kHStride);
+  P->o_h2 = cv.take(8 * (size_t)B * kHStride);
+  P->o_scale = cv.take(8 * (size_t)B * (P->m + 1));
   P->o_y = cv.take(8 * (size_t)B * kMaxRestart);
   P->o_lsq = cv.take(8 * (size_t)B * 3 * (kMaxRestart + 1));
   P->o_wn0 = cv.take(8 * (size_t)B);
@@ -217,7 +220,7 @@ static void layout(a2d_plan* P) {
 // ---------------------------------------------------------------------------
 __global__ void k_init_state(Batch b, double* U) {
   const Tile t = b.tiles[blockIdx.x];
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   const double rho = cs.winf[0], u = cs.winf[1], v = cs.winf[2], p = cs.winf[3];
   const double Uc[4] = {rho, rho * u, rho * v, p / kGm1 + 0.5 * rho * (u * u + v * v)};
@@ -403,23 +406,29 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
   launch_stencil<TV, true, double>(B, ta, s);
   // r = M t, v0 = r / ||r||
   precond<TJ>(P, B, t, r, NW, s);
-  launch_norm1(B, r, cpartn, NW, s);
-  NormalizeArgs<TB> n0;
-  n0.w = r;
-  n0.Vout = V;
-  n0.part_norm = cpartn;
-  n0.ctl = ctl;
-  n0.live = live;
-  n0.k = -1;
-  n0.need = NW;
-  launch_normalize<TB>(B, n0, s);
   double* h1 = P->at<double>(P->o_h1);
   double* h2 = P->at<double>(P->o_h2);
   double* wn0 = P->at<double>(P->o_wn0);
+  double* scale = P->at<double>(P->o_scale);
+  GsArgs<TB> g0;
+  g0.w = r;
+  g0.Vout = V;
+  g0.part_norm = cpartn;
+  g0.need = NW;
+  launch_gs_start<TB>(B, g0, s);
+  GsCloseArgs c0;
+  c0.part_norm = cpartn;
+  c0.scale = scale;
+  c0.ctl = ctl;
+  c0.live = live;
+  c0.k = -1;
+  c0.need = NW;
+  launch_gs_close(B, c0, s);
   for (int k = 0; k < P->m; ++k) {
     StencilArgs<TB> za;
     za.U = U;
     za.V = V + (size_t)k * vs;
+    za.vscale = scale + (size_t)k * P->ncases;
     za.diag = diag;
     za.out = z;
     za.lim_k = P->p.lim_k;
@@ -428,47 +437,49 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
     za.need = KR;
     launch_stencil<TV, true, TB>(B, za, s);
     precond<TJ>(P, B, z, w, KR, s);
-    // classical Gram-Schmidt, two passes
-    DotArgs<TB> d;
-    d.w = w;
-    d.V = V;
-    d.vstride = vs;
-    d.nq = k + 1;
-    d.with_norm = 1;
-    d.part = cpart;
-    d.pstride = P->pstride;
-    d.need = KR;
-    launch_dots<TB>(B, d, s);
-    UpdateArgs<TB> u;
-    u.w = w;
-    u.V = V;
-    u.vstride = vs;
-    u.nq = k + 1;
-    u.part = cpart;
-    u.pstride = P->pstride;
-    u.hstore = h1;
-    u.wn0 = wn0;
-    u.need = KR;
-    launch_update<TB>(B, u, s);
-    d.with_norm = 0;
-    launch_dots<TB>(B, d, s);
-    u.hstore = h2;
-    u.wn0 = nullptr;
-    u.part_norm = cpartn;
-    launch_update<TB>(B, u, s);
-    NormalizeArgs<TB> nk;
-    nk.w = w;
-    nk.Vout = V + (size_t)(k + 1) * vs;
-    nk.part_norm = cpartn;
-    nk.wn0 = wn0;
-    nk.h1 = h1;
-    nk.h2 = h2;
-    nk.H = P->at<double>(P->o_H);
-    nk.ctl = ctl;
-    nk.live = live;
-    nk.k = k;
-    nk.need = KR;
-    launch_normalize<TB>(B, nk, s);
+    // classical Gram-Schmidt run twice, three passes over the basis
+    GsArgs<TB> g;
+    g.w = w;
+    g.V = V;
+    g.vstride = vs;
+    g.nq = k + 1;
+    g.part = cpart;
+    g.pstride = P->pstride;
+    g.h1 = h1;
+    g.h2 = h2;
+    g.scale = scale;
+    g.Vout = V + (size_t)(k + 1) * vs;
+    g.part_norm = cpartn;
+    g.tmp = t;
+    g.need = KR;
+    g.with_norm = 1;
+    launch_gs_dots<TB>(B, g, s);
+    GsReduceArgs rd;
+    rd.part = cpart;
+    rd.pstride = P->pstride;
+    rd.nq = k + 1;
+    rd.scale = scale;
+    rd.h = h1;
+    rd.wn0 = wn0;
+    rd.need = KR;
+    launch_gs_reduce(B, rd, s);
+    launch_gs_project<TB>(B, g, s);
+    rd.h = h2;
+    rd.wn0 = nullptr;
+    launch_gs_reduce(B, rd, s);
+    launch_gs_finish<TB>(B, g, s);
+    GsCloseArgs ck;
+    ck.part_norm = cpartn;
+    ck.wn0 = wn0;
+    ck.h1 = h1;
+    ck.h2 = h2;
+    ck.H = P->at<double>(P->o_H);
+    ck.scale = scale;
+    ck.ctl = ctl;
+    ck.live = live;
+    ck.k = k;
+    ck.need = KR;
+    launch_gs_close(B, ck, s);
   }
   launch_lstsq(B, live, ctl, P->at<double>(P->o_H), P->at<double>(P->o_y), P->at<double>(P->o_lsq), s);
   CombineArgs<TB> ca;
@@ -476,6 +487,7 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
   ca.V = V;
   ca.vstride = vs;
   ca.y = P->at<double>(P->o_y);
+  ca.scale = scale;
   ca.ctl = ctl;
   ca.out = dU;
   ca.need = NW;
@@ -660,6 +672,8 @@ int a2d_plan_bind(a2d_plan* P, void* workspace, size_t bytes, void* stream) {
   if (P->host_count == nullptr) A2D_CK(cudaMallocHost(&P->host_count, sizeof(int)));
   k_reset<<<(P->ncases + 63) / 64, 64, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.cfl0);
   A2D_CK(cudaMemsetAsync(P->ws + P->o_circ_rk, 0, 8 * (size_t)P->ncases, s));
+  A2D_CK(gs_configure<double>());
+  A2D_CK(gs_configure<float>());
   A2D_CK(cudaGetLastError());
   return A2D_OK;
 }
@@ -901,54 +915,33 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
         else launch_rhs<double, double>(B, ra, s);
         break;
       }
-      case A2D_K_DOTS: {
-        if (mixed) {
-          DotArgs<float> d;
-          d.w = P->vec(kW);
-          d.V = P->at<float>(P->o_V);
-          d.vstride = vs;
-          d.nq = half;
-          d.with_norm = 1;
-          d.part = P->at<double>(P->o_cpart);
-          d.pstride = P->pstride;
-          launch_dots<float>(B, d, s);
-        } else {
-          DotArgs<double> d;
-          d.w = P->vec(kW);
-          d.V = P->at<double>(P->o_V);
-          d.vstride = vs;
-          d.nq = half;
-          d.with_norm = 1;
-          d.part = P->at<double>(P->o_cpart);
-          d.pstride = P->pstride;
-          launch_dots<double>(B, d, s);
-        }
-        break;
-      }
-      case A2D_K_UPDATE: {
-        if (mixed) {
-          UpdateArgs<float> u;
-          u.w = P->vec(kPA);
-          u.V = P->at<float>(P->o_V);
-          u.vstride = vs;
-          u.nq = half;
-          u.part = P->at<double>(P->o_cpart);
-          u.pstride = P->pstride;
-          u.hstore = P->at<double>(P->o_h1);
-          u.part_norm = P->at<double>(P->o_cpartn);
-          launch_update<float>(B, u, s);
-        } else {
-          UpdateArgs<double> u;
-          u.w = P->vec(kPA);
-          u.V = P->at<double>(P->o_V);
-          u.vstride = vs;
-          u.nq = half;
-          u.part = P->at<double>(P->o_cpart);
-          u.pstride = P->pstride;
-          u.hstore = P->at<double>(P->o_h1);
-          u.part_norm = P->at<double>(P->o_cpartn);
-          launch_update<double>(B, u, s);
-        }
+      case A2D_K_DOTS:
+      case A2D_K_UPDATE:
+      case A2D_K_PROJECT: {
+        // Gram-Schmidt passes with restart/2 basis vectors; the output vector is a
+        // scratch slot past the ones read
+        auto run = [&](auto* Vb) {
+          using TB = std::remove_pointer_t<decltype(Vb)>;
+          GsArgs<TB> g;
+          g.w = P->vec(kW);
+          g.V = Vb;
+          g.vstride = vs;
+          g.nq = half;
+          g.with_norm = 1;
+          g.part = P->at<double>(P->o_cpart);
+          g.pstride = P->pstride;
+          g.h1 = P->at<double>(P->o_h1);
+          g.h2 = P->at<double>(P->o_h2);
+          g.scale = P->at<double>(P->o_scale);
+          g.Vout = Vb + (size_t)P->m * vs;
+          g.part_norm = P->at<double>(P->o_cpartn);
+          g.tmp = P->vec(kPB);
+          if (which == A2D_K_DOTS) launch_gs_dots<TB>(B, g, s);
+          else if (which == A2D_K_PROJECT) launch_gs_project<TB>(B, g, s);
+          else launch_gs_finish<TB>(B, g, s);
+        };
+        if (mixed) run(P->at<float>(P->o_V));
+        else run(P->at<double>(P->o_V));
         break;
       }
       case A2D_K_RESIDUAL: {
@@ -995,7 +988,7 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
         break;
     }
   };
-  if (which < 0 || which > A2D_K_FACTOR) return fail(A2D_ERR_ARG, "time_kernel: unknown kernel");
+  if (which < 0 || which > A2D_K_PROJECT) return fail(A2D_ERR_ARG, "time_kernel: unknown kernel");
   cudaEvent_t e0, e1;
   A2D_CK(cudaEventCreate(&e0));
   A2D_CK(cudaEventCreate(&e1));

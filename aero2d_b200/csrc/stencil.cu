@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(256) k_stencil(Batch b, StencilArgs<VT> a) {
 
   const Tile t = b.tiles[blockIdx.x];
   if (!case_live(b, t.cs, a.need)) return;
-  const CaseDev& cs = b.cases[t.cs];
+  const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
   Metric<T> m{g};
   const int ni = g.ni, nc = g.nc;
@@ -342,10 +342,12 @@ __global__ void __launch_bounds__(256) k_stencil(Batch b, StencilArgs<VT> a) {
       R[k] = (sFi[k][jl][il + 1] - sFi[k][jl][il]) + (sFj[k][jl + 1][il] - sFj[k][jl][il]);
     if constexpr (LIN) {
       const T dg = a.diag != nullptr ? T(a.diag[cs.cell_off + (size_t)gj * ni + gi]) : T(0);
+      // the product is linear in V: a raw Krylov vector's scale applies to the result
+      const T vs = a.vscale != nullptr ? T(a.vscale[t.cs]) : T(1);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const size_t q = vidx(g, k, gj, gi);
-        T y = a.diag != nullptr ? dg * T(V[q]) + R[k] : R[k];
+        T y = (a.diag != nullptr ? dg * T(V[q]) + R[k] : R[k]) * vs;
         if (a.bvec != nullptr) y = T(a.bvec[base + q]) - y;
         a.out[base + q] = (double)y;
       }
@@ -376,7 +378,7 @@ __global__ void __launch_bounds__(256) k_forces(Batch b, const double* __restric
                                                 const CaseCtl* ctl, double* hist_cl, int hist_cap) {
   const int cs_id = blockIdx.x;
   if (!case_live(b, cs_id, 0)) return;
-  const CaseDev& cs = b.cases[cs_id];
+  const CaseDev cs = b.cases[cs_id];
   const GridDev& g = cs.g;
   const double* Uc = U + 4 * cs.cell_off;
   const double uinf = cs.winf[1], vinf = cs.winf[2], pinf = cs.winf[3];

@@ -172,6 +172,8 @@ def batch_solve(plan, max_iter):
     nsteps, done, frozen, lastrn, r0 = plan.status()
     conv = done & ~frozen
     lat = np.array([t_steps[n - 1] if n > 0 else 0.0 for n in nsteps])
+    batch_solve.last_step_ms = np.diff(np.concatenate([[0.0], t_steps]))
+    batch_solve.last_live = np.array([(nsteps > s).sum() for s in range(len(evs))])
     return float(t_steps[-1]), lat, nsteps, conv, frozen, len(evs)
 
 
@@ -188,10 +190,12 @@ def algorithmic_bytes(kernel: str, cells: int, restart: int, mixed: bool) -> flo
         "rhs": 4 * d + 4 * d + 16 * f + 16 * f + 16 * f + 4 * d,
         # U, V, diag, z, face vectors (2 i-face + 2 j-face components)
         "jvp": 4 * d + 4 * f + d + 4 * d + 4 * f,
-        # w, restart/2 basis vectors
+        # Gram-Schmidt pass 1: w, restart/2 basis vectors
         "dots": 4 * d + half * 4 * f,
-        # w (load + store), restart/2 basis vectors
-        "update": 8 * d + half * 4 * f,
+        # pass 2: w, restart/2 basis vectors read once (kept on chip for the re-projection)
+        "project": 4 * d + half * 4 * f,
+        # pass 3: w, restart/2 basis vectors, the next basis vector written
+        "update": 4 * d + half * 4 * f + 4 * f,
     }[kernel]
     return float(per_cell) * cells
 
@@ -199,7 +203,7 @@ def algorithmic_bytes(kernel: str, cells: int, restart: int, mixed: bool) -> flo
 def launches_per_step(kernel: str, restart: int, sweeps: int = 4) -> int:
     napp = restart + 2
     return {"lines": sweeps * napp, "rhs": (sweeps - 1) * napp, "jvp": restart + 1,
-            "dots": 2 * restart, "update": 2 * restart}[kernel]
+            "dots": restart, "project": restart, "update": restart}[kernel]
 
 
 def read_traffic(kernel: str):
@@ -275,6 +279,11 @@ def gpu_arm(args, rank: int, world: int, dist):
         c = torch.tensor([float(converged)], dtype=torch.float64, device=dev)
         dist.all_reduce(c, op=dist.ReduceOp.SUM)
         elapsed_ms, converged = float(t.item()), int(c.item())
+    step_ms, live = batch_solve.last_step_ms, batch_solve.last_live
+    step_profile = {"ms_per_newton_step_by_live_cases": {
+        f"{lo}-{hi}": round(float(step_ms[(live >= lo) & (live <= hi)].mean()), 3)
+        for lo, hi in ((B * 3 // 4 + 1, B), (B // 4 + 1, B * 3 // 4), (2, B // 4), (1, 1))
+        if ((live >= lo) & (live <= hi)).any()}}
     lat = np.concatenate([r[1][r[3]] for r in runs]) if converged else np.array([np.nan])
     nsteps_mix = runs[-1][2]
     coef_mix = plan.forces()[0].cpu().numpy()
@@ -295,6 +304,7 @@ def gpu_arm(args, rank: int, world: int, dist):
         "converged_cases": converged,
         "cases_total": B * args.steps * world,
         "newton_steps_mean": round(float(nsteps_mix.mean()), 2),
+        "step_profile": step_profile,
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 2), "p95": round(float(np.percentile(lat, 95)), 2),
                        "p99": round(float(np.percentile(lat, 99)), 2),
                        "note": "per converged case, from batch start to its retirement"},
@@ -338,7 +348,7 @@ def gpu_arm(args, rank: int, world: int, dist):
     # ---- roofline of the dominant kernel (CUDA events on the plan's stream) --
     cells = B * 256 * 64
     kernels = {"lines": _lib.K_LINES, "rhs": _lib.K_RHS, "jvp": _lib.K_JVP, "dots": _lib.K_DOTS,
-               "update": _lib.K_UPDATE}
+               "project": _lib.K_PROJECT, "update": _lib.K_UPDATE}
     ktimes = {k: plan.time_kernel(v, reps=20) for k, v in kernels.items()}
     share = {k: ktimes[k] * launches_per_step(k, args.restart) for k in kernels}
     dom = max(share, key=share.get)
@@ -417,6 +427,24 @@ def reference_arm(args):
             "e2e": {"value": round(value, 5), "unit": "cases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def profile_driver(args):
+    """A short run for ncu: the plan of the bench workload (--cases of it),
+    `--profile` Newton steps from the freestream."""
+    import torch
+    from aero2d_b200.euler import EulerSolver
+    from aero2d_b200.implicit import ImplicitEuler
+    from aero2d_b200.plan import Plan
+    dev = torch.device("cuda", 0)
+    machs, alphas = draw_cases(SEED, args.cases)
+    base = EulerSolver(make_grid(), dtype=np.float64 if args.fp64 else np.float32, device=dev)
+    s = ImplicitEuler(base, gmres_restart=args.restart)
+    plan = Plan([base.dgrid] * args.cases, base.freestream(machs, alphas), s.params(args.tol, args.max_iter), dev)
+    plan.init_freestream()
+    for _ in range(args.profile):
+        plan.newton_step()
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -430,7 +458,13 @@ def main():
     ap.add_argument("--single-sample", type=int, default=4)
     ap.add_argument("--cpu-procs", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", type=int, default=0, metavar="STEPS",
+                    help="profiling driver: build the mixed plan, run STEPS Newton steps, print nothing")
+    ap.add_argument("--fp64", action="store_true", help="with --profile: the all-FP64 plan")
     args = ap.parse_args()
+    if args.profile:
+        profile_driver(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -141,11 +141,12 @@ int a2d_plan_stats(const a2d_plan* plan, int* kernels_per_step, int* steps_taken
 #define A2D_K_JVP 0        /* linearised residual stencil on the whole batch            */
 #define A2D_K_LINES 1      /* sequential block-Thomas recurrences of one sweep          */
 #define A2D_K_RHS 2        /* parallel right-hand side of a coupled sweep               */
-#define A2D_K_DOTS 3       /* Gram-Schmidt projections against restart/2 basis vectors */
-#define A2D_K_UPDATE 4     /* Gram-Schmidt subtraction with restart/2 basis vectors     */
+#define A2D_K_DOTS 3       /* Gram-Schmidt pass 1: projections on restart/2 vectors     */
+#define A2D_K_UPDATE 4     /* Gram-Schmidt pass 3: subtraction, next basis vector       */
 #define A2D_K_RESIDUAL 5   /* FP64 residual stencil                                     */
 #define A2D_K_FACEJAC 6    /* first-order face Jacobian blocks                          */
 #define A2D_K_FACTOR 7     /* block-Thomas factorisation                                */
+#define A2D_K_PROJECT 8    /* Gram-Schmidt pass 2: subtraction and re-projection        */
 /* times `reps` back-to-back launches of one kernel on the plan's current data with CUDA
  * events on `stream`, for every case of the plan; *ms receives the mean per launch.
  * Overwrites scratch vectors only (not U). Synchronises. */
