@@ -101,6 +101,7 @@ SIGNATURES = {
     "a2d_smooth": (_I, [_P, _P]),
     "a2d_set_circulation": (_I, [_P, C.POINTER(_D), _P]),
     "a2d_hllc_flux": (_I, [_I, _P, _P, _P, _P, _P]),
+    "a2d_residual_norms_static": (_I, [_P, _I, _I, _I, _P, _P, _P, C.POINTER(Params), _P, _P, _P]),
 }
 
 _lib = None

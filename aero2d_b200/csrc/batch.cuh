@@ -102,6 +102,39 @@ struct Batch {
   int ncases, ntiles, nchunks, ngroups;
 };
 
+// Layout of a grid's metrics blob: FP64 vol, Si, Sj, xf, yf, xw, yw, then (from the
+// next 256-byte boundary) FP32 copies of vol, Si, Sj, xf, yf.
+__host__ __device__ inline size_t metrics_doubles(int ni, int nc) {
+  return 5 * (size_t)ni * nc + 6 * (size_t)ni;
+}
+__host__ __device__ inline size_t metrics_floats(int ni, int nc) {
+  return 5 * (size_t)ni * nc + 4 * (size_t)ni;
+}
+__host__ __device__ inline size_t metrics_float_offset(int ni, int nc) {
+  return (metrics_doubles(ni, nc) * 8 + 255) & ~size_t(255);
+}
+__host__ __device__ inline GridDev grid_view(const void* blob, int ni, int nc) {
+  GridDev g;
+  g.ni = ni;
+  g.nc = nc;
+  const size_t N = (size_t)ni * nc;
+  const double* d = static_cast<const double*>(blob);
+  g.vol = d;
+  g.Si = d + N;
+  g.Sj = g.Si + 2 * N;
+  g.xf = g.Sj + 2 * (N + ni);
+  g.yf = g.xf + ni;
+  g.xw = g.yf + ni;
+  g.yw = g.xw + ni;
+  const float* f = reinterpret_cast<const float*>(static_cast<const char*>(blob) + metrics_float_offset(ni, nc));
+  g.vol_f = f;
+  g.Si_f = f + N;
+  g.Sj_f = g.Si_f + 2 * N;
+  g.xf_f = g.Sj_f + 2 * (N + ni);
+  g.yf_f = g.xf_f + ni;
+  return g;
+}
+
 // metric accessors in the compute precision
 template <typename T> struct Metric;
 template <> struct Metric<double> {

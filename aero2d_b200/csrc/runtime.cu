@@ -29,7 +29,7 @@ namespace a2d {
 
 thread_local std::string g_last_error;
 
-static int fail(int code, const std::string& msg) {
+int fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
@@ -51,39 +51,8 @@ struct Carve {
   }
 };
 
-static size_t metrics_doubles(int ni, int nc) {
-  const size_t N = (size_t)ni * nc;
-  return 5 * N + 6 * (size_t)ni;
-}
-static size_t metrics_floats(int ni, int nc) {
-  const size_t N = (size_t)ni * nc;
-  return 5 * N + 4 * (size_t)ni;
-}
 static size_t metrics_total_bytes(int ni, int nc) {
-  return ((metrics_doubles(ni, nc) * 8 + 255) & ~size_t(255)) + metrics_floats(ni, nc) * 4;
-}
-
-static GridDev grid_view(const void* blob, int ni, int nc) {
-  GridDev g;
-  g.ni = ni;
-  g.nc = nc;
-  const size_t N = (size_t)ni * nc;
-  const double* d = static_cast<const double*>(blob);
-  g.vol = d;
-  g.Si = d + N;
-  g.Sj = g.Si + 2 * N;
-  g.xf = g.Sj + 2 * (N + ni);
-  g.yf = g.xf + ni;
-  g.xw = g.yf + ni;
-  g.yw = g.xw + ni;
-  const float* f = reinterpret_cast<const float*>(static_cast<const char*>(blob) +
-                                                  ((metrics_doubles(ni, nc) * 8 + 255) & ~size_t(255)));
-  g.vol_f = f;
-  g.Si_f = f + N;
-  g.Sj_f = g.Si_f + 2 * N;
-  g.xf_f = g.Sj_f + 2 * (N + ni);
-  g.yf_f = g.xf_f + ni;
-  return g;
+  return metrics_float_offset(ni, nc) + metrics_floats(ni, nc) * 4;
 }
 
 enum VecSlot { kU = 0, kR, kVin, kJV, kDU, kB, kX0, kT, kRr, kZ, kW, kPA, kPB, kU0, kNumVec };
@@ -594,8 +563,7 @@ int a2d_metrics_build(int ni, int nj, const double* x, const double* y, void* me
     return fail(A2D_ERR_ARG, "metrics: bad arguments");
   const int nc = nj - 1;
   double* md = static_cast<double*>(metrics);
-  float* mf = reinterpret_cast<float*>(static_cast<char*>(metrics) +
-                                       ((metrics_doubles(ni, nc) * 8 + 255) & ~size_t(255)));
+  float* mf = reinterpret_cast<float*>(static_cast<char*>(metrics) + metrics_float_offset(ni, nc));
   launch_metrics(ni, nc, x, y, md, mf, static_cast<cudaStream_t>(stream));
   A2D_CK(cudaGetLastError());
   return A2D_OK;

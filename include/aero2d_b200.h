@@ -161,6 +161,27 @@ int a2d_smooth(a2d_plan* plan, void* stream);
 /* per-case circulation slot used by a2d_rk_iterate: host array [ncases] */
 int a2d_set_circulation(a2d_plan* plan, const double* circ, void* stream);
 
+/* ---- residual without device allocation ---- */
+/* No counterpart in the reference: an entry point for callers that cannot call cudaMalloc
+ * (a host application whose memory manager owns all device memory and does not let a plugin
+ * allocate, or a loop that must not allocate while it runs).  It computes, for ncases cases
+ * on one grid, R = residual(U, winf, circ) exactly as a2d_residual does and the per-case
+ * residual norm rnorm[k] = sqrt(mean((R_rho / vol)^2)) that the Newton loop tests for
+ * convergence.  It allocates nothing: besides the caller's buffers it uses one file-scope
+ * device array of about 0.86 MB, which every GPU that loads the library holds until the process
+ * exits; the first call on a device looks up that array's address, so make the first call on
+ * each device before any stream capture.  Calls share the array, so calls whose kernels overlap
+ * on the GPU race.  Limits: ncases <= 64, 4 <= ni <= 512, 2 <= nj - 1 <= 128; larger batches are
+ * rejected with A2D_ERR_ARG.
+ *   metrics: the grid's blob from a2d_metrics_build; U, R: device [ncases][4][nj-1][ni]
+ *   (component, wall-normal, circumferential: the library's internal layout, i fastest);
+ *   winf: device [ncases][4]; circ: device [ncases] or NULL for Gamma(U) = Cl(U) M / 2;
+ *   params: host, NULL for defaults (lim_k, order, vortex_correction are used);
+ *   rnorm: device [ncases]. */
+int a2d_residual_norms_static(const void* metrics, int ni, int nj, int ncases, const double* U,
+                              const double* winf, const double* circ, const a2d_params* params,
+                              double* R, double* rnorm, void* stream);
+
 /* point-wise HLLC flux of n faces (euler.py:79-121): WL, WR [4][n], S [2][n], F [4][n]
  * device FP64 arrays */
 int a2d_hllc_flux(int n, const double* WL, const double* WR, const double* S, double* F, void* stream);
