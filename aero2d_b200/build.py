@@ -26,6 +26,9 @@ OBJ = ROOT / "_build" / "obj"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+# The FP32 linearisation of the mixed-precision solver uses approximate FP32
+# division and square root; every FP64 kernel keeps IEEE-exact arithmetic.
+EXTRA = {"stencil_fp32.cu": ["--prec-div=false", "--prec-sqrt=false", "--ftz=true"]}
 
 
 def nvcc() -> str:
@@ -50,7 +53,7 @@ def _stale() -> bool:
 def _compile(src: Path, verbose: bool) -> Path:
     OBJ.mkdir(parents=True, exist_ok=True)
     obj = OBJ / (src.stem + ".o")
-    cmd = [nvcc(), *ARCH, *FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *FLAGS, *EXTRA.get(src.name, []), f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
