@@ -93,6 +93,26 @@ __device__ __forceinline__ void stv(double* p, const double (&v)[4]) {
   *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
 }
 
+// four consecutive basis entries in their storage precision
+template <typename TB> struct Raw4;
+template <> struct Raw4<float> {
+  float4 v;
+  __device__ __forceinline__ void load(const float* p) { v = *reinterpret_cast<const float4*>(p); }
+  __device__ __forceinline__ double operator[](int u) const {
+    return u == 0 ? v.x : (u == 1 ? v.y : (u == 2 ? v.z : v.w));
+  }
+};
+template <> struct Raw4<double> {
+  double2 a, b;
+  __device__ __forceinline__ void load(const double* p) {
+    a = *reinterpret_cast<const double2*>(p);
+    b = *reinterpret_cast<const double2*>(p + 2);
+  }
+  __device__ __forceinline__ double operator[](int u) const {
+    return u == 0 ? a.x : (u == 1 ? a.y : (u == 2 ? b.x : b.y));
+  }
+};
+
 // pass 1 (and the re-projection of the chained path) ---------------------------
 template <typename TB, int NQ>
 __global__ void __launch_bounds__(kGB) k_gs_dots(Batch b, GsArgs<TB> a) {
@@ -105,23 +125,20 @@ __global__ void __launch_bounds__(kGB) k_gs_dots(Batch b, GsArgs<TB> a) {
   double acc[NQ + 1];
 #pragma unroll
   for (int q = 0; q <= NQ; ++q) acc[q] = 0.0;
-#pragma unroll
-  for (int s = 0; s < kGE / 4; ++s) {
-    const int e = 4 * (threadIdx.x + s * kGB);
+#pragma unroll 1
+  for (int s = 0; s < kGE; ++s) {
+    const int e = threadIdx.x + s * kGB;
     if (e < ch.len) {
-      double w[4];
-      ldv(a.w + base + e, w);
+      const double w = a.w[base + e];
+      // every load is issued unconditionally (slots past nq re-read the last
+      // vector) so that all of them are in flight together; only the sums are guarded
+      TB v[NQ];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        if (q < a.nq) {
-          double v[4];
-          ldv(V + (size_t)q * a.vstride + e, v);
+      for (int q = 0; q < NQ; ++q) v[q] = V[(size_t)(q < a.nq ? q : a.nq - 1) * a.vstride + e];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) acc[q] += v[u] * w[u];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) acc[NQ] += w[u] * w[u];
+      for (int q = 0; q < NQ; ++q)
+        if (q < a.nq) acc[q] += (double)v[q] * w;
+      acc[NQ] += w * w;
     }
   }
   const double r = gs_reduce_to_thread<NQ + 1>(acc, scratch);
@@ -132,47 +149,34 @@ __global__ void __launch_bounds__(kGB) k_gs_dots(Batch b, GsArgs<TB> a) {
 
 // pass 2, fused: w' = w - V (s h1), then V . w' --------------------------------
 template <typename TB, int NQ>
-__global__ void __launch_bounds__(kGB, 2) k_gs_project(Batch b, GsArgs<TB> a) {
+__global__ void __launch_bounds__(kGB) k_gs_project(Batch b, GsArgs<TB> a) {
   const Chunk ch = b.chunks[blockIdx.x];
   if (!case_live(b, ch.cs, a.need)) return;
   const CaseDev cs = b.cases[ch.cs];
   const size_t base = 4 * cs.cell_off + ch.begin;
   __shared__ double coef[NQ];
   __shared__ double scratch[8 * NQ];
-  // per-thread slots for the basis entries used twice: [q][thread] pairs in
-  // storage precision (written and read back by the same thread only)
-  extern __shared__ unsigned char gs_dyn[];
-  using Pair = typename std::conditional<sizeof(TB) == 4, float2, double2>::type;
-  Pair* keep = reinterpret_cast<Pair*>(gs_dyn);
+  // the basis entries are used twice and stay in registers, in storage precision
   coef_to_smem(a, ch.cs, b.ncases, coef, false);
   const TB* V = a.V + base;
   double acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
 #pragma unroll 1
-  for (int s = 0; s < kGE / 2; ++s) {
-    const int e = 2 * (threadIdx.x + s * kGB);
+  for (int s = 0; s < kGE; ++s) {
+    const int e = threadIdx.x + s * kGB;
     if (e < ch.len) {
-      double sub0 = 0.0, sub1 = 0.0;
+      TB v[NQ];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        if (q < a.nq) {
-          const Pair p = *reinterpret_cast<const Pair*>(V + (size_t)q * a.vstride + e);
-          keep[q * kGB + threadIdx.x] = p;
-          sub0 += (double)p.x * coef[q];
-          sub1 += (double)p.y * coef[q];
-        }
-      }
-      double w[2];
-      ldv(a.w + base + e, w);
-      const double wp0 = w[0] - sub0, wp1 = w[1] - sub1;
+      for (int q = 0; q < NQ; ++q) v[q] = V[(size_t)(q < a.nq ? q : a.nq - 1) * a.vstride + e];
+      double sub = 0.0;
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        if (q < a.nq) {
-          const Pair p = keep[q * kGB + threadIdx.x];
-          acc[q] += (double)p.x * wp0 + (double)p.y * wp1;
-        }
-      }
+      for (int q = 0; q < NQ; ++q)
+        if (q < a.nq) sub += (double)v[q] * coef[q];
+      const double wp = a.w[base + e] - sub;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q)
+        if (q < a.nq) acc[q] += (double)v[q] * wp;
     }
   }
   const double r = gs_reduce_to_thread<NQ>(acc, scratch);
@@ -191,18 +195,19 @@ __global__ void __launch_bounds__(kGB) k_gs_sub(Batch b, GsArgs<TB> a) {
   coef_to_smem(a, ch.cs, b.ncases, coef, a.both != 0);
   const TB* V = a.V + (size_t)a.q0 * a.vstride + base;
   double nrm = 0.0;
-#pragma unroll
+#pragma unroll 1
   for (int s = 0; s < kGE / 4; ++s) {
     const int e = 4 * (threadIdx.x + s * kGB);
     if (e < ch.len) {
       double sub[4] = {0.0, 0.0, 0.0, 0.0};
+      Raw4<TB> v[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) v[q].load(V + (size_t)(q < a.nq ? q : a.nq - 1) * a.vstride + e);
 #pragma unroll
       for (int q = 0; q < NQ; ++q) {
         if (q < a.nq) {
-          double v[4];
-          ldv(V + (size_t)q * a.vstride + e, v);
 #pragma unroll
-          for (int u = 0; u < 4; ++u) sub[u] += v[u] * coef[q];
+          for (int u = 0; u < 4; ++u) sub[u] += v[q][u] * coef[q];
         }
       }
       double w[4];
@@ -301,47 +306,19 @@ __global__ void k_gs_close(Batch b, GsCloseArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int kSlice = 32;
 
-// dynamic shared memory of pass 2 for a tier: one entry pair per vector and thread
-template <typename TB, int NQ>
-constexpr size_t project_smem() {
-  return (size_t)NQ * kGB * 2 * sizeof(TB);
-}
-
-#define A2D_GS_DISPATCH(KERNEL, SMEM)                                                      \
+#define A2D_GS_DISPATCH(KERNEL)                                                            \
   template <typename TB>                                                                   \
   static void dispatch_##KERNEL(const Batch& b, const GsArgs<TB>& a, cudaStream_t s) {     \
     if (!b.nchunks) return;                                                                \
-    if (a.nq <= 8) KERNEL<TB, 8><<<b.nchunks, kGB, SMEM(8), s>>>(b, a);                     \
-    else if (a.nq <= 16) KERNEL<TB, 16><<<b.nchunks, kGB, SMEM(16), s>>>(b, a);             \
-    else if (a.nq <= 24) KERNEL<TB, 24><<<b.nchunks, kGB, SMEM(24), s>>>(b, a);             \
-    else KERNEL<TB, 32><<<b.nchunks, kGB, SMEM(32), s>>>(b, a);                             \
+    if (a.nq <= 8) KERNEL<TB, 8><<<b.nchunks, kGB, 0, s>>>(b, a);                           \
+    else if (a.nq <= 16) KERNEL<TB, 16><<<b.nchunks, kGB, 0, s>>>(b, a);                    \
+    else if (a.nq <= 24) KERNEL<TB, 24><<<b.nchunks, kGB, 0, s>>>(b, a);                    \
+    else KERNEL<TB, 32><<<b.nchunks, kGB, 0, s>>>(b, a);                                    \
   }
-#define A2D_NO_SMEM(N) 0
-#define A2D_PROJECT_SMEM(N) project_smem<TB, N>()
-A2D_GS_DISPATCH(k_gs_dots, A2D_NO_SMEM)
-A2D_GS_DISPATCH(k_gs_project, A2D_PROJECT_SMEM)
-A2D_GS_DISPATCH(k_gs_sub, A2D_NO_SMEM)
+A2D_GS_DISPATCH(k_gs_dots)
+A2D_GS_DISPATCH(k_gs_project)
+A2D_GS_DISPATCH(k_gs_sub)
 #undef A2D_GS_DISPATCH
-#undef A2D_NO_SMEM
-#undef A2D_PROJECT_SMEM
-
-// allows the pass-2 tiers their dynamic shared memory (once per process and type)
-template <typename TB>
-cudaError_t gs_configure() {
-  cudaError_t e = cudaSuccess;
-  cudaError_t r;
-  if ((r = cudaFuncSetAttribute(k_gs_project<TB, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)project_smem<TB, 8>())) != cudaSuccess) e = r;
-  if ((r = cudaFuncSetAttribute(k_gs_project<TB, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)project_smem<TB, 16>())) != cudaSuccess) e = r;
-  if ((r = cudaFuncSetAttribute(k_gs_project<TB, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)project_smem<TB, 24>())) != cudaSuccess) e = r;
-  if ((r = cudaFuncSetAttribute(k_gs_project<TB, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)project_smem<TB, 32>())) != cudaSuccess) e = r;
-  return e;
-}
-template cudaError_t gs_configure<double>();
-template cudaError_t gs_configure<float>();
 
 template <typename TB>
 void launch_gs_dots(const Batch& b, const GsArgs<TB>& a0, cudaStream_t s) {

@@ -60,7 +60,5 @@ template <typename TB> void launch_gs_project(const Batch& b, const GsArgs<TB>& 
 template <typename TB> void launch_gs_finish(const Batch& b, const GsArgs<TB>& a, cudaStream_t s);
 template <typename TB> void launch_gs_start(const Batch& b, const GsArgs<TB>& a, cudaStream_t s);
 void launch_gs_close(const Batch& b, const GsCloseArgs& a, cudaStream_t s);
-// grants the pass-2 kernels their dynamic shared memory; call before launching them
-template <typename TB> cudaError_t gs_configure();
 
 }  // namespace a2d

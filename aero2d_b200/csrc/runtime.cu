@@ -640,8 +640,6 @@ int a2d_plan_bind(a2d_plan* P, void* workspace, size_t bytes, void* stream) {
   if (P->host_count == nullptr) A2D_CK(cudaMallocHost(&P->host_count, sizeof(int)));
   k_reset<<<(P->ncases + 63) / 64, 64, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.cfl0);
   A2D_CK(cudaMemsetAsync(P->ws + P->o_circ_rk, 0, 8 * (size_t)P->ncases, s));
-  A2D_CK(gs_configure<double>());
-  A2D_CK(gs_configure<float>());
   A2D_CK(cudaGetLastError());
   return A2D_OK;
 }
