@@ -23,7 +23,7 @@ A2D_MIXED = 1
 VEC_U, VEC_R, VEC_V, VEC_JV, VEC_DU = 0, 1, 2, 3, 4
 
 # kernels that a2d_time_kernel can time
-K_JVP, K_LINES, K_RHS, K_DOTS, K_UPDATE, K_RESIDUAL, K_FACEJAC, K_FACTOR, K_PROJECT = range(9)
+K_JVP, K_SWEEP, K_SWEEP_FIRST, K_DOTS, K_UPDATE, K_RESIDUAL, K_FACEJAC, K_FACTOR, K_PROJECT = range(9)
 
 
 class ExtensionMissing(RuntimeError):

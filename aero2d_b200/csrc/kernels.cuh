@@ -46,25 +46,28 @@ struct FactorArgs {
   void* INV = nullptr;             // inverse of the block-Thomas pivots [rows nc]
   void* CF = nullptr;              // upper factors c_j                 [rows nc]
   void* G = nullptr;               // -inv_j A_j                         [rows nc]
+  void* P = nullptr;               // inv_j JIL(i)   (coupling to line i-1) [rows nc]
+  void* Q = nullptr;               // inv_j JIR(i+1) (coupling to line i+1) [rows nc]
   double* diag = nullptr;          // per-cell vol / dtau
   double cfl_base = 2.5;           // EulerSolver.cfl, which local_dt multiplies and step() divides out
   uint32_t need = 0;
 };
 
-struct RhsArgs {
-  const double* r = nullptr;       // right-hand side of the preconditioner
-  const double* xprev = nullptr;   // previous sweep (nullptr on the first sweep)
-  double* out = nullptr;           // e = inv (r - off)
+// One line-Jacobi sweep x = M_line^-1 (r - off(xprev)), with the factors of
+// k_factor.  The first sweep (no previous iterate) computes e0 = inv r and may
+// keep it for the later sweeps, whose right-hand side is e0 + P xprev[i-1] -
+// Q xprev[i+1].
+struct SweepArgs {
+  const double* r = nullptr;       // first sweep: right-hand side
+  double* e0 = nullptr;            // first sweep: inv r written when set; later sweeps: read
+  const double* xprev = nullptr;   // later sweeps: previous iterate (must not alias x)
+  double* x = nullptr;             // result (the first sweep may write it over r)
   const void* INV = nullptr;
-  const void* JIL = nullptr;
-  const void* JIR = nullptr;
-  uint32_t need = 0;
-};
-
-struct LinesArgs {
-  double* x = nullptr;             // in: e, out: the line solution (in place)
+  const void* P = nullptr;
+  const void* Q = nullptr;
   const void* G = nullptr;
   const void* CF = nullptr;
+  uint32_t* err = nullptr;         // set to 1 when a copy wait runs out of time
   uint32_t need = 0;
 };
 
@@ -83,10 +86,11 @@ void launch_face_jac(const Batch& b, const JacArgs& a, cudaStream_t s);
 template <typename TJ, typename TF>
 void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s);
 
-template <typename TJ, typename TF>
-void launch_rhs(const Batch& b, const RhsArgs& a, cudaStream_t s);
+// one line-Jacobi sweep (sweep.cu); FIRST: the sweep without i-coupling
+template <typename TF, bool FIRST>
+void launch_sweep(const Batch& b, const SweepArgs& a, cudaStream_t s);
 
-template <typename TF>
-void launch_lines(const Batch& b, const LinesArgs& a, cudaStream_t s);
+// raises the dynamic shared-memory limit of the sweep kernels (host, once per device)
+cudaError_t sweep_init();
 
 }  // namespace a2d

@@ -8,22 +8,14 @@
 //               block-Thomas forward elimination along each wall-normal line
 //               in FP64: den_j = D_j - A_j c_{j-1}, inv_j = den_j^-1,
 //               c_j = inv_j C_j (aero2d/implicit.py:81-128), and stores inv_j,
-//               c_j and G_j = -inv_j A_j.  One thread per line, 32 lines (one
-//               warp) per line group.
-//  k_rhs        first half of a line-Jacobi sweep (aero2d/implicit.py:150-157):
-//               moves the i-coupling of the previous sweep to the right-hand
-//               side and applies inv_j, e_j = inv_j (r_j - off_j); fully
-//               parallel over cells.
-//  k_lines      second half: the sequential recurrences d_j = e_j + G_j d_{j-1}
-//               and x_j = d_j - c_j x_{j+1} along each line
-//               (aero2d/implicit.py:130-148), which equal the reference's
-//               d_j = inv_j (r_j - A_j d_{j-1}) in exact arithmetic.  Only 20
-//               words per step remain on the sequential path, loaded 4 steps
-//               ahead.
+//               c_j, G_j = -inv_j A_j and the premultiplied i-couplings
+//               P_j = inv_j JIL(i), Q_j = inv_j JIR(i+1) of the sweeps.  One
+//               thread per line, 32 lines (one warp) per line group.
+// The sweeps themselves are in sweep.cu.
 //
-// The blocks are stored lane-blocked ([group][row][entry][lane]) so that at
-// every step of the sequential j recurrence a warp reads each matrix entry of
-// its 32 lines as one coalesced 256 B (FP64) or 128 B (FP32) transaction.
+// The blocks are stored lane-blocked ([group][row][entry][lane]): the blocks
+// of one line group at one row j are one contiguous run, which the sweep
+// kernel streams with bulk copies.
 #include "batch.cuh"
 #include "kernels.cuh"
 #include "physics.cuh"
@@ -206,6 +198,20 @@ __device__ __forceinline__ void load_block(const TJ* base, long long row0, int r
   for (int e = 0; e < 16; ++e) A[e] = (double)base[lbidx(row0, rows, g, j, e, lane)];
 }
 
+// out = A B (4x4, FP64), stored in TF at lane-blocked entries q0 + e * kLanes
+template <typename TF>
+__device__ __forceinline__ void mul4_store(const double A[16], const double B[16], TF* out, size_t q0) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      double s = A[r * 4 + 0] * B[0 * 4 + c];
+#pragma unroll
+      for (int k = 1; k < 4; ++k) s += A[r * 4 + k] * B[k * 4 + c];
+      out[q0 + (size_t)(r * 4 + c) * kLanes] = TF(s);
+    }
+}
+
 template <typename TJ, typename TF>
 __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -227,6 +233,8 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   TF* INV = static_cast<TF*>(a.INV);
   TF* CF = static_cast<TF*>(a.CF);
   TF* G = static_cast<TF*>(a.G);
+  TF* P = static_cast<TF*>(a.P);
+  TF* Q = static_cast<TF*>(a.Q);
   const double* U = a.U + 4 * cs.cell_off;
   const double cfl = a.ctl[grp.cs].cfl;
   double cprev[16];
@@ -317,158 +325,11 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
       CF[q] = TF(cprev[e]);
       G[q] = TF(D[e]);
     }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// right-hand side of one line-Jacobi sweep, fully parallel over cells:
-//   e = inv_j (r - off),  off = Bim x[i-1] + Bip x[i+1] = -(JIL x[i-1]) + JIR(i+1) x[i+1]
-// (off = 0 on the first sweep).  One thread per cell, 32 x 8 cells per CTA.
-// ---------------------------------------------------------------------------
-template <typename TJ, typename TF>
-__global__ void __launch_bounds__(256) k_rhs(Batch b, RhsArgs a) {
-  const Tile t = b.tiles[blockIdx.x];
-  if (!case_live(b, t.cs, a.need)) return;
-  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
-  if (lane >= t.ti || row >= t.tj) return;
-  const CaseDev cs = b.cases[t.cs];
-  const GridDev& g = cs.g;
-  const int ni = g.ni, nc = g.nc;
-  const int i = t.i0 + lane, j = t.j0 + row, grp = t.i0 / kLanes;
-  const size_t base = 4 * cs.cell_off;
-  double rhs[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) rhs[k] = a.r[base + vidx(g, k, j, i)];
-  if (a.xprev != nullptr) {
-    const int ip = (i + 1 == ni) ? 0 : i + 1;
-    const int im = (i == 0) ? ni - 1 : i - 1;
-    const double* xp = a.xprev + base;
-    double xm4[4], xp4[4], AL[16], AR[16];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      xm4[k] = xp[vidx(g, k, j, im)];
-      xp4[k] = xp[vidx(g, k, j, ip)];
-    }
-    load_block(static_cast<const TJ*>(a.JIL), cs.rows_nc, nc, grp, j, lane, AL);
-    load_block(static_cast<const TJ*>(a.JIR), cs.rows_nc, nc, ip / kLanes, j, ip % kLanes, AR);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      double s1 = AL[q * 4 + 0] * xm4[0];
-      double s2 = AR[q * 4 + 0] * xp4[0];
-#pragma unroll
-      for (int k = 1; k < 4; ++k) {
-        s1 += AL[q * 4 + k] * xm4[k];
-        s2 += AR[q * 4 + k] * xp4[k];
-      }
-      rhs[q] = rhs[q] - (-s1 + s2);
-    }
-  }
-  double IV[16];
-  load_block(static_cast<const TF*>(a.INV), cs.rows_nc, nc, grp, j, lane, IV);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    double s = IV[q * 4 + 0] * rhs[0];
-#pragma unroll
-    for (int k = 1; k < 4; ++k) s += IV[q * 4 + k] * rhs[k];
-    a.out[base + vidx(g, q, j, i)] = s;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// the sequential part of the block-Thomas solve, in place on x:
-//   forward   d_j = e_j + G_j d_{j-1}
-//   backward  x_j = d_j - C_j x_{j+1}
-// Four threads per line, one per row of the 4x4 blocks; the quad exchanges
-// the previous step's 4-vector by shuffles.  Each thread keeps the operands of
-// its row for the next kAhead steps in registers (one FP64 vector entry and
-// four block entries per step), so a step waits on 1/kAhead of the memory
-// latency, and a 32-line group fills four warps.
-// ---------------------------------------------------------------------------
-constexpr int kAhead = 8;
-
-template <typename TF>
-struct RowStep {
-  double v;
-  TF m[4];
-};
-
-template <typename TF>
-__device__ __forceinline__ void load_row(RowStep<TF>& s, const double* x, const TF* M, const CaseDev& cs,
-                                         const GridDev& g, int grp, int lane, int i, int q, int j) {
-  if (j < 0 || j >= g.nc) return;
-  s.v = x[vidx(g, q, j, i)];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) s.m[c] = M[lbidx(cs.rows_nc, g.nc, grp, j, q * 4 + c, lane)];
-}
-
-// the 4 components of the quad's current vector, from the quad's lanes
-__device__ __forceinline__ void quad_gather(double mine, int base, double out[4]) {
-#pragma unroll
-  for (int c = 0; c < 4; ++c) out[c] = __shfl_sync(0xffffffffu, mine, base | c);
-}
-
-// one CTA of 128 threads per 32-line group: warp w holds lines 8w..8w+7,
-// lane 4l+q is row q of line l
-template <typename TF>
-__global__ void __launch_bounds__(128) k_lines(Batch b, LinesArgs a) {
-  const int gid = blockIdx.x;
-  if (gid >= b.ngroups) return;
-  const Group grp = b.groups[gid];
-  if (!case_live(b, grp.cs, a.need)) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int l = warp * 8 + (lane >> 2);       // line within the group
-  const int q = lane & 3;                      // row of the 4x4 blocks owned
-  const int base = lane & ~3;                  // first lane of the quad
-  const bool owner = l < grp.n;                // quads past the group's last line only shuffle
-  const int ll = owner ? l : grp.n - 1;        // their loads stay on a valid line
-  const CaseDev cs = b.cases[grp.cs];
-  const GridDev& g = cs.g;
-  const int nc = g.nc;
-  const int i = grp.i0 + ll;
-  double* x = a.x + 4 * cs.cell_off;
-  const TF* G = static_cast<const TF*>(a.G);
-  const TF* CF = static_cast<const TF*>(a.CF);
-  RowStep<TF> buf[kAhead];
-  // forward: d_j = e_j + G_j d_{j-1}
-  double d = 0.0;
-#pragma unroll
-  for (int u = 0; u < kAhead; ++u) load_row(buf[u], x, G, cs, g, grp.g, ll, i, q, u);
-  for (int j0 = 0; j0 < nc; j0 += kAhead) {
-#pragma unroll
-    for (int u = 0; u < kAhead; ++u) {
-      const int j = j0 + u;
-      if (j < nc) {
-        double dp[4];
-        quad_gather(d, base, dp);
-        double acc = buf[u].v;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc += (double)buf[u].m[c] * dp[c];
-        d = acc;
-        if (owner) x[vidx(g, q, j, i)] = acc;
-        load_row(buf[u], x, G, cs, g, grp.g, ll, i, q, j + kAhead);
-      }
-    }
-  }
-  // backward: x_j = d_j - C_j x_{j+1}
-  double xn = 0.0;
-  const int top = nc - 1;
-#pragma unroll
-  for (int u = 0; u < kAhead; ++u) load_row(buf[u], x, CF, cs, g, grp.g, ll, i, q, top - u);
-  for (int j0 = top; j0 >= 0; j0 -= kAhead) {
-#pragma unroll
-    for (int u = 0; u < kAhead; ++u) {
-      const int j = j0 - u;
-      if (j >= 0) {
-        double xp[4];
-        quad_gather(xn, base, xp);
-        double acc = 0.0;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc += (double)buf[u].m[c] * xp[c];
-        xn = buf[u].v - acc;
-        if (owner) x[vidx(g, q, j, i)] = xn;
-        load_row(buf[u], x, CF, cs, g, grp.g, ll, i, q, j - kAhead);
-      }
-    }
+    // i-coupling of the sweeps, premultiplied: P = inv JIL(i), Q = inv JIR(i+1)
+    load_block(JIL, cs.rows_nc, nc, grp.g, j, lane, T1);
+    mul4_store(inv, T1, P, lbidx(cs.rows_nc, nc, grp.g, j, 0, lane));
+    load_block(JIR, cs.rows_nc, nc, gp, j, lp, T1);
+    mul4_store(inv, T1, Q, lbidx(cs.rows_nc, nc, grp.g, j, 0, lane));
   }
 }
 
@@ -482,24 +343,10 @@ void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s) {
   if (b.ngroups == 0) return;
   k_factor<TJ, TF><<<(b.ngroups + 3) / 4, 128, 0, s>>>(b, a);
 }
-template <typename TJ, typename TF>
-void launch_rhs(const Batch& b, const RhsArgs& a, cudaStream_t s) {
-  if (b.ntiles == 0) return;
-  k_rhs<TJ, TF><<<b.ntiles, 256, 0, s>>>(b, a);
-}
-template <typename TF>
-void launch_lines(const Batch& b, const LinesArgs& a, cudaStream_t s) {
-  if (b.ngroups == 0) return;
-  k_lines<TF><<<b.ngroups, 128, 0, s>>>(b, a);
-}
 
 template void launch_face_jac<double>(const Batch&, const JacArgs&, cudaStream_t);
 template void launch_face_jac<float>(const Batch&, const JacArgs&, cudaStream_t);
 template void launch_factor<double, double>(const Batch&, const FactorArgs&, cudaStream_t);
 template void launch_factor<float, float>(const Batch&, const FactorArgs&, cudaStream_t);
-template void launch_rhs<double, double>(const Batch&, const RhsArgs&, cudaStream_t);
-template void launch_rhs<float, float>(const Batch&, const RhsArgs&, cudaStream_t);
-template void launch_lines<double>(const Batch&, const LinesArgs&, cudaStream_t);
-template void launch_lines<float>(const Batch&, const LinesArgs&, cudaStream_t);
 
 }  // namespace a2d

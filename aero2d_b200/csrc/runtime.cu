@@ -55,7 +55,7 @@ static size_t metrics_total_bytes(int ni, int nc) {
   return metrics_float_offset(ni, nc) + metrics_floats(ni, nc) * 4;
 }
 
-enum VecSlot { kU = 0, kR, kVin, kJV, kDU, kB, kX0, kT, kRr, kZ, kW, kPA, kPB, kU0, kNumVec };
+enum VecSlot { kU = 0, kR, kVin, kJV, kDU, kB, kX0, kT, kRr, kZ, kW, kPA, kPB, kU0, kPE, kNumVec };
 
 }  // namespace a2d
 
@@ -76,7 +76,7 @@ struct a2d_plan {
   // workspace layout (offsets)
   size_t o_cases = 0, o_tiles = 0, o_chunks = 0, o_groups = 0, o_cpoff = 0, o_live = 0, o_ctl = 0;
   size_t o_vec[kNumVec] = {};
-  size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_G = 0, o_V = 0;
+  size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_G = 0, o_P = 0, o_Q = 0, o_V = 0;
   size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_lsq = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
   size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0;
   int pstride = 0;
@@ -162,6 +162,8 @@ static void layout(a2d_plan* P) {
   P->o_INV = cv.take(P->tj * lb * P->rows_nc);
   P->o_CF = cv.take(P->tj * lb * P->rows_nc);
   P->o_G = cv.take(P->tj * lb * P->rows_nc);
+  P->o_P = cv.take(P->tj * lb * P->rows_nc);
+  P->o_Q = cv.take(P->tj * lb * P->rows_nc);
   P->o_V = cv.take(P->tb * 4 * C * (size_t)(P->m + 1));
   P->o_H = cv.take(8 * (size_t)B * kMaxRestart * (kMaxRestart + 1));
   P->o_h1 = cv.take(8 * (size_t)B * kHStride);
@@ -180,7 +182,7 @@ static void layout(a2d_plan* P) {
   P->o_cp = cv.take(8 * (size_t)P->total_ni);
   P->o_hrn = cv.take(8 * (size_t)B * P->p.max_iter);
   P->o_hcl = cv.take(8 * (size_t)B * P->p.max_iter);
-  P->o_cnt = cv.take(8);
+  P->o_cnt = cv.take(8);   // [0] live-case count, [1] sweep copy-wait failure flag
   P->bytes = cv.off + 256;
 }
 
@@ -266,29 +268,52 @@ __global__ void k_point_flux(int n, const double* WL, const double* WR, const do
 // ---------------------------------------------------------------------------
 namespace a2d {
 
+static SweepArgs sweep_args(const a2d_plan* P, uint32_t need) {
+  SweepArgs a;
+  a.INV = P->at<void>(P->o_INV);
+  a.P = P->at<void>(P->o_P);
+  a.Q = P->at<void>(P->o_Q);
+  a.G = P->at<void>(P->o_G);
+  a.CF = P->at<void>(P->o_CF);
+  a.err = P->at<uint32_t>(P->o_cnt) + 1;
+  a.need = need;
+  return a;
+}
+
+static FactorArgs factor_args(const a2d_plan* P, uint32_t need) {
+  FactorArgs fa;
+  fa.U = P->vec(kU);
+  fa.ctl = P->ctl();
+  fa.JIL = P->at<void>(P->o_JIL);
+  fa.JIR = P->at<void>(P->o_JIR);
+  fa.JJL = P->at<void>(P->o_JJL);
+  fa.JJR = P->at<void>(P->o_JJR);
+  fa.INV = P->at<void>(P->o_INV);
+  fa.CF = P->at<void>(P->o_CF);
+  fa.G = P->at<void>(P->o_G);
+  fa.P = P->at<void>(P->o_P);
+  fa.Q = P->at<void>(P->o_Q);
+  fa.diag = P->at<double>(P->o_diag);
+  fa.cfl_base = P->p.cfl;
+  fa.need = need;
+  return fa;
+}
+
+// x = M^-1 r: jacobi_sweeps line-Jacobi sweeps (aero2d/implicit.py:150-157);
+// rin may be dst
 template <typename TJ>
 static void precond(a2d_plan* P, const Batch& B, const double* rin, double* dst, uint32_t need, cudaStream_t s) {
-  RhsArgs ra;
-  ra.r = rin;
-  ra.INV = P->at<void>(P->o_INV);
-  ra.JIL = P->at<void>(P->o_JIL);
-  ra.JIR = P->at<void>(P->o_JIR);
-  ra.need = need;
-  LinesArgs la;
-  la.G = P->at<void>(P->o_G);
-  la.CF = P->at<void>(P->o_CF);
-  la.need = need;
+  SweepArgs a = sweep_args(P, need);
   const int sweeps = std::max(1, P->p.jacobi_sweeps);
   double* bufs[2] = {P->vec(kPA), P->vec(kPB)};
-  const double* prev = nullptr;
-  for (int sw = 0; sw < sweeps; ++sw) {
-    double* out = (sw == sweeps - 1) ? dst : bufs[sw & 1];
-    ra.xprev = prev;
-    ra.out = out;
-    launch_rhs<TJ, TJ>(B, ra, s);
-    la.x = out;
-    launch_lines<TJ>(B, la, s);
-    prev = out;
+  a.r = rin;
+  a.e0 = sweeps > 1 ? P->vec(kPE) : nullptr;
+  a.x = sweeps > 1 ? bufs[0] : dst;
+  launch_sweep<TJ, true>(B, a, s);
+  for (int sw = 1; sw < sweeps; ++sw) {
+    a.xprev = a.x;
+    a.x = (sw == sweeps - 1) ? dst : bufs[sw & 1];
+    launch_sweep<TJ, false>(B, a, s);
   }
 }
 
@@ -304,20 +329,7 @@ static void precond_setup(a2d_plan* P, const Batch& B, uint32_t need, cudaStream
   ja.vortex = P->p.vortex_correction;
   ja.need = need;
   launch_face_jac<TJ>(B, ja, s);
-  FactorArgs fa;
-  fa.U = P->vec(kU);
-  fa.ctl = P->ctl();
-  fa.JIL = ja.JIL;
-  fa.JIR = ja.JIR;
-  fa.JJL = ja.JJL;
-  fa.JJR = ja.JJR;
-  fa.INV = P->at<void>(P->o_INV);
-  fa.CF = P->at<void>(P->o_CF);
-  fa.G = P->at<void>(P->o_G);
-  fa.diag = P->at<double>(P->o_diag);
-  fa.cfl_base = P->p.cfl;
-  fa.need = need;
-  launch_factor<TJ, TJ>(B, fa, s);
+  launch_factor<TJ, TJ>(B, factor_args(P, need), s);
 }
 
 static StencilArgs<double> residual_args(a2d_plan* P) {
@@ -637,7 +649,9 @@ int a2d_plan_bind(a2d_plan* P, void* workspace, size_t bytes, void* stream) {
   B.ntiles = (int)P->tiles.size();
   B.nchunks = (int)P->chunks.size();
   B.ngroups = (int)P->groups.size();
-  if (P->host_count == nullptr) A2D_CK(cudaMallocHost(&P->host_count, sizeof(int)));
+  if (P->host_count == nullptr) A2D_CK(cudaMallocHost(&P->host_count, 2 * sizeof(int)));
+  A2D_CK(cudaMemsetAsync(P->ws + P->o_cnt, 0, 8, s));
+  A2D_CK(sweep_init());
   k_reset<<<(P->ncases + 63) / 64, 64, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.cfl0);
   A2D_CK(cudaMemsetAsync(P->ws + P->o_circ_rk, 0, 8 * (size_t)P->ncases, s));
   A2D_CK(cudaGetLastError());
@@ -799,8 +813,9 @@ int a2d_newton_run(a2d_plan* P, int max_steps, int* steps, void* stream) {
     P->steps_taken += 1;
     ++done;
     k_count<<<1, 256, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.retire, dcount);
-    A2D_CK(cudaMemcpyAsync(P->host_count, dcount, sizeof(int), cudaMemcpyDeviceToHost, s));
+    A2D_CK(cudaMemcpyAsync(P->host_count, dcount, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     A2D_CK(cudaStreamSynchronize(s));
+    if (P->host_count[1] != 0) return fail(A2D_ERR_CUDA, "line sweep: a bulk-copy wait ran out of time");
     if (*P->host_count == 0) break;
   }
   if (steps != nullptr) *steps = done;
@@ -813,8 +828,9 @@ int a2d_live_count(a2d_plan* P, int* n, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int* dcount = P->at<int>(P->o_cnt);
   k_count<<<1, 256, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.retire, dcount);
-  A2D_CK(cudaMemcpyAsync(P->host_count, dcount, sizeof(int), cudaMemcpyDeviceToHost, s));
+  A2D_CK(cudaMemcpyAsync(P->host_count, dcount, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   A2D_CK(cudaStreamSynchronize(s));
+  if (P->host_count[1] != 0) return fail(A2D_ERR_CUDA, "line sweep: a bulk-copy wait ran out of time");
   *n = *P->host_count;
   return A2D_OK;
 }
@@ -860,25 +876,22 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
         }
         break;
       }
-      case A2D_K_LINES: {
-        LinesArgs la;
-        la.G = P->at<void>(P->o_G);
-        la.CF = P->at<void>(P->o_CF);
-        la.x = P->vec(kPA);
-        if (mixed) launch_lines<float>(B, la, s);
-        else launch_lines<double>(B, la, s);
+      case A2D_K_SWEEP: {
+        SweepArgs a = sweep_args(P, 0);
+        a.e0 = P->vec(kPE);
+        a.xprev = P->vec(kPB);
+        a.x = P->vec(kPA);
+        if (mixed) launch_sweep<float, false>(B, a, s);
+        else launch_sweep<double, false>(B, a, s);
         break;
       }
-      case A2D_K_RHS: {
-        RhsArgs ra;
-        ra.r = P->vec(kZ);
-        ra.xprev = P->vec(kPB);
-        ra.out = P->vec(kPA);
-        ra.INV = P->at<void>(P->o_INV);
-        ra.JIL = P->at<void>(P->o_JIL);
-        ra.JIR = P->at<void>(P->o_JIR);
-        if (mixed) launch_rhs<float, float>(B, ra, s);
-        else launch_rhs<double, double>(B, ra, s);
+      case A2D_K_SWEEP_FIRST: {
+        SweepArgs a = sweep_args(P, 0);
+        a.r = P->vec(kZ);
+        a.e0 = P->vec(kPE);
+        a.x = P->vec(kPA);
+        if (mixed) launch_sweep<float, true>(B, a, s);
+        else launch_sweep<double, true>(B, a, s);
         break;
       }
       case A2D_K_DOTS:
@@ -933,18 +946,7 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
           if (mixed) launch_face_jac<float>(B, ja, s);
           else launch_face_jac<double>(B, ja, s);
         } else {
-          FactorArgs fa;
-          fa.U = P->vec(kU);
-          fa.ctl = P->ctl();
-          fa.JIL = ja.JIL;
-          fa.JIR = ja.JIR;
-          fa.JJL = ja.JJL;
-          fa.JJR = ja.JJR;
-          fa.INV = P->at<void>(P->o_INV);
-          fa.CF = P->at<void>(P->o_CF);
-          fa.G = P->at<void>(P->o_G);
-          fa.diag = P->at<double>(P->o_diag);
-          fa.cfl_base = P->p.cfl;
+          const FactorArgs fa = factor_args(P, 0);
           if (mixed) launch_factor<float, float>(B, fa, s);
           else launch_factor<double, double>(B, fa, s);
         }

@@ -184,10 +184,11 @@ def algorithmic_bytes(kernel: str, cells: int, restart: int, mixed: bool) -> flo
     d = 8
     half = max(1, restart // 2)
     per_cell = {
-        # e, G, d(store), d(load), CF, x(store)
-        "lines": 4 * d + 16 * f + 4 * d + 4 * d + 16 * f + 4 * d,
-        # r, x_prev, JIL, JIR, INV, e
-        "rhs": 4 * d + 4 * d + 16 * f + 16 * f + 16 * f + 4 * d,
+        # coupled line sweep: e0, x_prev, P, Q, G, C, x (store); the d_j written by
+        # the forward recurrence and read back by the backward one is not counted
+        "sweep": 4 * d + 4 * d + 4 * 16 * f + 4 * d,
+        # first sweep: r, inv, G, C, e0 (store), x (store)
+        "sweep_first": 4 * d + 3 * 16 * f + 4 * d + 4 * d,
         # U, V, diag, z, face vectors (2 i-face + 2 j-face components)
         "jvp": 4 * d + 4 * f + d + 4 * d + 4 * f,
         # Gram-Schmidt pass 1: w, restart/2 basis vectors
@@ -202,7 +203,7 @@ def algorithmic_bytes(kernel: str, cells: int, restart: int, mixed: bool) -> flo
 
 def launches_per_step(kernel: str, restart: int, sweeps: int = 4) -> int:
     napp = restart + 2
-    return {"lines": sweeps * napp, "rhs": (sweeps - 1) * napp, "jvp": restart + 1,
+    return {"sweep": (sweeps - 1) * napp, "sweep_first": napp, "jvp": restart + 1,
             "dots": restart, "project": restart, "update": restart}[kernel]
 
 
@@ -347,7 +348,7 @@ def gpu_arm(args, rank: int, world: int, dist):
 
     # ---- roofline of the dominant kernel (CUDA events on the plan's stream) --
     cells = B * 256 * 64
-    kernels = {"lines": _lib.K_LINES, "rhs": _lib.K_RHS, "jvp": _lib.K_JVP, "dots": _lib.K_DOTS,
+    kernels = {"sweep": _lib.K_SWEEP, "sweep_first": _lib.K_SWEEP_FIRST, "jvp": _lib.K_JVP, "dots": _lib.K_DOTS,
                "project": _lib.K_PROJECT, "update": _lib.K_UPDATE}
     ktimes = {k: plan.time_kernel(v, reps=20) for k, v in kernels.items()}
     share = {k: ktimes[k] * launches_per_step(k, args.restart) for k in kernels}

@@ -139,8 +139,9 @@ int a2d_plan_stats(const a2d_plan* plan, int* kernels_per_step, int* steps_taken
 
 /* ---- measurement ---- */
 #define A2D_K_JVP 0        /* linearised residual stencil on the whole batch            */
-#define A2D_K_LINES 1      /* sequential block-Thomas recurrences of one sweep          */
-#define A2D_K_RHS 2        /* parallel right-hand side of a coupled sweep               */
+#define A2D_K_SWEEP 1      /* one coupled line-Jacobi sweep (right-hand side + both     */
+                           /* block-Thomas recurrences, fused)                          */
+#define A2D_K_SWEEP_FIRST 2 /* the first sweep of a preconditioner application         */
 #define A2D_K_DOTS 3       /* Gram-Schmidt pass 1: projections on restart/2 vectors     */
 #define A2D_K_UPDATE 4     /* Gram-Schmidt pass 3: subtraction, next basis vector       */
 #define A2D_K_RESIDUAL 5   /* FP64 residual stencil                                     */

@@ -120,10 +120,14 @@ def test_jvp_vs_complex_step(cuda, prec, tol):
         assert err < tol, (k, err)
 
 
-def test_precond_vs_oracle(cuda):
-    g = grid("0012", 33, 25)
+# ni = 64 fills two 32-line groups; ni = 80 leaves a partial third group.
+# Tolerances: FP64 factors 1e-10 relative; FP32-stored factors (mixed) 1e-4.
+@pytest.mark.parametrize("ns,nj,sweeps,mixed", [(33, 25, 4, False), (41, 17, 1, False), (41, 17, 2, False),
+                                                (41, 17, 4, False), (41, 17, 4, True), (33, 25, 3, True)])
+def test_precond_vs_oracle(cuda, ns, nj, sweeps, mixed):
+    g = grid("0012", ns, nj)
     om = EulerModel(g.x, g.y)
-    im = ImplicitModel(om)
+    im = ImplicitModel(om, jacobi_sweeps=sweeps)
     w = om.freestream(0.55, 1.0)
     U = perturbed_state(om, w, seed=2, amp=0.01)
     cfl = 37.0
@@ -134,14 +138,17 @@ def test_precond_vs_oracle(cuda):
     fac = im.factor_lines(D, Bjm, Bjp)
     r = np.random.default_rng(9).standard_normal(U.shape)
     xo = im.precond(fac, Bim, Bip, r)
-    pl, _ = _plan(g, [w], cuda)
+    over = {"jacobi_sweeps": sweeps}
+    if mixed:
+        over["precision"] = _lib.A2D_MIXED
+    pl, _ = _plan(g, [w], cuda, **over)
     pl.set_vec(_lib.VEC_U, 0, torch.as_tensor(U))
     pl.set_cfl([cfl])
     pl.precond_setup()
     pl.set_vec(_lib.VEC_V, 0, torch.as_tensor(r))
     pl.precond_apply()
     x = pl.get_vec(_lib.VEC_JV, 0).cpu().numpy()
-    assert np.max(np.abs(x - xo)) / np.max(np.abs(xo)) < 1e-10
+    assert np.max(np.abs(x - xo)) / np.max(np.abs(xo)) < (1e-4 if mixed else 1e-10)
 
 
 def test_smoothing_vs_fft(cuda):
