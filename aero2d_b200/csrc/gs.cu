@@ -5,8 +5,8 @@
 //   pass 1  k_gs_dots     raw projections V_raw[q] . w and w . w, per chunk
 //   reduce  k_gs_reduce   per case, fixed chunk order: h1_q = s_q (V_raw[q] . w)
 //   pass 2  k_gs_project  w' = w - sum_q V_raw[q] s_q h1_q and V_raw[q] . w' from one
-//                         read of the basis (the entry's basis values stay in
-//                         registers between the subtraction and the projection)
+//                         read of the basis (the sub-tile stays in shared memory
+//                         between the subtraction and the projection)
 //   reduce  k_gs_reduce   h2_q
 //   pass 3  k_gs_sub      w'' = w - sum_q V_raw[q] s_q (h1_q + h2_q), written as the
 //                         next raw basis vector, with its squared norm
@@ -14,9 +14,10 @@
 //                         eps ||w|| (jax.scipy.sparse.linalg.gmres semantics), the
 //                         Hessenberg column and s_{k+1} = 1 / ||w''||
 //
-// Each thread handles kGE entries of a 4096-entry chunk against up to 32 basis
-// vectors held in registers (the count is a template tier NQ of 8, 16, 24 or
-// 32), so a chunk needs a single block reduction.  Bases of more than 32
+// The three passes stream a 4096-entry chunk per CTA through shared memory by
+// bulk copies (see "streaming passes" below); a thread keeps one partial sum
+// per basis vector in registers (the count is a template tier NQ of 8, 16, 24
+// or 32), so a chunk needs a single block reduction.  Bases of more than 32
 // vectors are processed in slices of 32 by chained launches.  Basis vectors
 // are stored unnormalised with their scale s_q, so no normalisation pass is
 // needed; w' is never stored, since pass 3 subtracts h1 + h2 from the
@@ -26,6 +27,7 @@
 
 #include "batch.cuh"
 #include "gs.cuh"
+#include "tma.cuh"
 
 namespace a2d {
 
@@ -93,137 +95,312 @@ __device__ __forceinline__ void stv(double* p, const double (&v)[4]) {
   *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
 }
 
-// four consecutive basis entries in their storage precision
-template <typename TB> struct Raw4;
-template <> struct Raw4<float> {
-  float4 v;
-  __device__ __forceinline__ void load(const float* p) { v = *reinterpret_cast<const float4*>(p); }
-  __device__ __forceinline__ double operator[](int u) const {
-    return u == 0 ? v.x : (u == 1 ? v.y : (u == 2 ? v.z : v.w));
+// ---------------------------------------------------------------------------
+// streaming passes.  A CTA of kGT threads owns one chunk and walks it in
+// sub-tiles of E entries; the E entries of w and of every basis vector of the
+// slice for one sub-tile (one stage) arrive by bulk copies on one mbarrier,
+// through a ring of as many stages as the shared-memory budget holds, issued
+// by thread 0 as soon as a stage is free.  Thread t works on entries
+// t*EPT .. t*EPT+EPT-1 of each sub-tile and keeps one partial sum per basis
+// vector in registers (NQ >= nq of them, a template tier); the chunk ends with
+// one fixed-order block reduction, so the result does not depend on which
+// other cases share the batch.
+// ---------------------------------------------------------------------------
+constexpr int kGT = 256;
+constexpr int kGsMaxStages = 8;
+constexpr size_t kGsSmemBudget = 72 * 1024;     // three CTAs per SM
+constexpr int kGsHeader = 128;                  // mbarriers and abort flags before the stages
+
+template <typename TB> struct GsTile;
+// 2 KB runs of every basis vector per stage (measured: larger runs beat deeper
+// rings; three CTAs per SM beat one CTA with more stages)
+template <> struct GsTile<float> { static constexpr int E = 512; };
+template <> struct GsTile<double> { static constexpr int E = 256; };
+
+template <typename TB>
+__host__ __device__ inline uint32_t gs_stage_bytes(int nq) {
+  return (uint32_t)GsTile<TB>::E * (uint32_t)(nq * sizeof(TB) + 8);
+}
+static_assert(kGsSmemBudget >= (size_t)GsTile<float>::E * (32 * 4 + 8) &&
+                  kGsSmemBudget >= (size_t)GsTile<double>::E * (32 * 8 + 8),
+              "one stage of a 32-vector slice must fit the shared-memory budget");
+
+template <typename TB>
+__host__ __device__ inline int gs_stages(int nq) {
+  const int s = (int)(kGsSmemBudget / gs_stage_bytes<TB>(nq));
+  return s < 1 ? 1 : (s > kGsMaxStages ? kGsMaxStages : s);
+}
+
+// fixed-order reduction of NV values over the kGT threads; thread t < NV receives value t
+template <int NV>
+__device__ __forceinline__ double gs_block_reduce(double (&v)[NV], double* scratch /* (kGT/32)*NV */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
   }
+  __syncthreads();   // the scratch may alias the last stage, still read above
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) scratch[warp * NV + q] = v[q];
+  }
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < NV) {
+#pragma unroll
+    for (int w = 0; w < kGT / 32; ++w) s += scratch[w * NV + threadIdx.x];
+  }
+  return s;
+}
+
+// EPT consecutive entries in their storage precision, from shared memory
+template <typename TB, int EPT> struct VecOf;
+template <> struct VecOf<float, 1> { using type = float; };
+template <> struct VecOf<float, 2> { using type = float2; };
+template <> struct VecOf<float, 4> { using type = float4; };
+template <> struct VecOf<double, 1> { using type = double; };
+template <> struct VecOf<double, 2> { using type = double2; };
+struct alignas(16) Double4x { double2 lo, hi; };
+template <> struct VecOf<double, 4> { using type = Double4x; };
+
+template <typename TB, int EPT>
+struct Entries {
+  alignas(sizeof(typename VecOf<TB, EPT>::type)) TB v[EPT];
+  __device__ __forceinline__ void load(const TB* p) {
+    using V = typename VecOf<TB, EPT>::type;
+    *reinterpret_cast<V*>(v) = *reinterpret_cast<const V*>(p);
+  }
+  __device__ __forceinline__ double operator[](int u) const { return (double)v[u]; }
 };
-template <> struct Raw4<double> {
-  double2 a, b;
-  __device__ __forceinline__ void load(const double* p) {
-    a = *reinterpret_cast<const double2*>(p);
-    b = *reinterpret_cast<const double2*>(p + 2);
+
+// the ring of one streaming pass over a chunk
+template <typename TB>
+struct GsRing {
+  static constexpr int E = GsTile<TB>::E;
+  static constexpr int EPT = E / kGT;
+  unsigned char* stages;
+  uint64_t* full;
+  int* abort;
+  int S, nq, len, nsub;
+  uint32_t stage_bytes;
+  const TB* V;        // first vector of the slice, at the chunk's first entry
+  size_t vstride;
+  const double* w;    // at the chunk's first entry
+
+  __device__ void init(unsigned char* smem, const GsArgs<TB>& a, const Chunk& ch, size_t base) {
+    full = reinterpret_cast<uint64_t*>(smem);
+    abort = reinterpret_cast<int*>(smem + 8 * kGsMaxStages);
+    stages = smem + kGsHeader;
+    nq = a.nq;
+    S = gs_stages<TB>(nq);
+    stage_bytes = gs_stage_bytes<TB>(nq);
+    len = ch.len;
+    nsub = (len + E - 1) / E;
+    V = a.V + (size_t)a.q0 * a.vstride + base;
+    vstride = a.vstride;
+    w = a.w + base;
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
+      mbar_init_fence();
+      abort[0] = abort[1] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int u = 0; u < S; ++u) issue(u);
   }
-  __device__ __forceinline__ double operator[](int u) const {
-    return u == 0 ? a.x : (u == 1 ? a.y : (u == 2 ? b.x : b.y));
+  // sub-tile u: entries u*E .. of the chunk (len is a multiple of 4 entries, so
+  // every copy is a multiple of 16 bytes)
+  __device__ void issue(int u) const {
+    if (u >= nsub) return;
+    const int e0 = u * E;
+    const int n = min(E, len - e0);
+    const int s = u % S;
+    unsigned char* st = stages + (size_t)s * stage_bytes;
+    mbar_arrive_expect(&full[s], (uint32_t)n * (uint32_t)(nq * sizeof(TB) + 8));
+    for (int q = 0; q < nq; ++q)
+      bulk_load(st + (size_t)q * E * sizeof(TB), V + (size_t)q * vstride + e0, n * sizeof(TB), &full[s]);
+    bulk_load(st + (size_t)nq * E * sizeof(TB), w + e0, n * 8, &full[s]);
+  }
+  __device__ const TB* vec(int u, int q) const {
+    return reinterpret_cast<const TB*>(stages + (size_t)(u % S) * stage_bytes) + (size_t)q * E;
+  }
+  __device__ const double* wvec(int u) const {
+    return reinterpret_cast<const double*>(stages + (size_t)(u % S) * stage_bytes + (size_t)nq * E * sizeof(TB));
+  }
+  __device__ void wait(int u) const {
+    if (!mbar_wait(&full[u % S], (u / S) & 1)) abort[u & 1] = 1;
+  }
+  // after consuming sub-tile u: frees its stage; false once a wait has run out
+  __device__ bool release(int u) const {
+    __syncthreads();
+    if (abort[u & 1]) return false;
+    if (threadIdx.x == 0) issue(u + S);
+    return true;
+  }
+  // error exit: record the failure and give the copies in flight a bounded time
+  __device__ void drain(int u, uint32_t* err) const {
+    if (threadIdx.x == 0) {
+      if (err != nullptr) atomicExch(err, 1u);
+      for (int v = u; v < u + S && v < nsub; ++v) (void)mbar_wait(&full[v % S], (v / S) & 1);
+    }
+    __syncthreads();
   }
 };
 
 // pass 1 (and the re-projection of the chained path) ---------------------------
 template <typename TB, int NQ>
-__global__ void __launch_bounds__(kGB) k_gs_dots(Batch b, GsArgs<TB> a) {
+__global__ void __launch_bounds__(kGT) k_gs_dots(Batch b, GsArgs<TB> a) {
+  extern __shared__ __align__(128) unsigned char smem[];
   const Chunk ch = b.chunks[blockIdx.x];
   if (!case_live(b, ch.cs, a.need)) return;
   const CaseDev cs = b.cases[ch.cs];
-  const size_t base = 4 * cs.cell_off + ch.begin;
-  __shared__ double scratch[8 * (NQ + 1)];
-  const TB* V = a.V + (size_t)a.q0 * a.vstride + base;
+  GsRing<TB> ring;
+  ring.init(smem, a, ch, 4 * cs.cell_off + ch.begin);
+  constexpr int EPT = GsRing<TB>::EPT;
   double acc[NQ + 1];
 #pragma unroll
   for (int q = 0; q <= NQ; ++q) acc[q] = 0.0;
+  const int nq = a.nq;
 #pragma unroll 1
-  for (int s = 0; s < kGE; ++s) {
-    const int e = threadIdx.x + s * kGB;
-    if (e < ch.len) {
-      const double w = a.w[base + e];
-      // every load is issued unconditionally (slots past nq re-read the last
-      // vector) so that all of them are in flight together; only the sums are guarded
-      TB v[NQ];
+  for (int u = 0; u < ring.nsub; ++u) {
+    ring.wait(u);
+    const int e = threadIdx.x * EPT;
+    if (e < ring.len - u * GsRing<TB>::E) {
+      const double* ws = ring.wvec(u) + e;
+      double w[EPT];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) v[q] = V[(size_t)(q < a.nq ? q : a.nq - 1) * a.vstride + e];
+      for (int t = 0; t < EPT; ++t) w[t] = ws[t];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q)
-        if (q < a.nq) acc[q] += (double)v[q] * w;
-      acc[NQ] += w * w;
+      for (int q = 0; q < NQ; ++q) {
+        Entries<TB, EPT> v;
+        v.load(ring.vec(u, q < nq ? q : nq - 1) + e);
+        if (q < nq) {
+#pragma unroll
+          for (int t = 0; t < EPT; ++t) acc[q] += v[t] * w[t];
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < EPT; ++t) acc[NQ] += w[t] * w[t];
+    }
+    if (!ring.release(u)) {
+      ring.drain(u, a.err);
+      return;
     }
   }
-  const double r = gs_reduce_to_thread<NQ + 1>(acc, scratch);
+  const double r = gs_block_reduce<NQ + 1>(acc, reinterpret_cast<double*>(ring.stages));
   double* part = a.part + (size_t)blockIdx.x * a.pstride;
-  if (threadIdx.x < a.nq) part[a.q0 + threadIdx.x] = r;
+  if (threadIdx.x < nq) part[a.q0 + threadIdx.x] = r;
   if (a.with_norm && threadIdx.x == NQ) part[a.norm_slot] = r;
 }
 
 // pass 2, fused: w' = w - V (s h1), then V . w' --------------------------------
 template <typename TB, int NQ>
-__global__ void __launch_bounds__(kGB) k_gs_project(Batch b, GsArgs<TB> a) {
+__global__ void __launch_bounds__(kGT) k_gs_project(Batch b, GsArgs<TB> a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double coef[NQ];
   const Chunk ch = b.chunks[blockIdx.x];
   if (!case_live(b, ch.cs, a.need)) return;
   const CaseDev cs = b.cases[ch.cs];
-  const size_t base = 4 * cs.cell_off + ch.begin;
-  __shared__ double coef[NQ];
-  __shared__ double scratch[8 * NQ];
-  // the basis entries are used twice and stay in registers, in storage precision
   coef_to_smem(a, ch.cs, b.ncases, coef, false);
-  const TB* V = a.V + base;
+  GsRing<TB> ring;
+  ring.init(smem, a, ch, 4 * cs.cell_off + ch.begin);
+  constexpr int EPT = GsRing<TB>::EPT;
   double acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+  const int nq = a.nq;
 #pragma unroll 1
-  for (int s = 0; s < kGE; ++s) {
-    const int e = threadIdx.x + s * kGB;
-    if (e < ch.len) {
-      TB v[NQ];
+  for (int u = 0; u < ring.nsub; ++u) {
+    ring.wait(u);
+    const int e = threadIdx.x * EPT;
+    if (e < ring.len - u * GsRing<TB>::E) {
+      const double* ws = ring.wvec(u) + e;
+      double sub[EPT];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) v[q] = V[(size_t)(q < a.nq ? q : a.nq - 1) * a.vstride + e];
-      double sub = 0.0;
+      for (int t = 0; t < EPT; ++t) sub[t] = 0.0;
 #pragma unroll
-      for (int q = 0; q < NQ; ++q)
-        if (q < a.nq) sub += (double)v[q] * coef[q];
-      const double wp = a.w[base + e] - sub;
+      for (int q = 0; q < NQ; ++q) {
+        Entries<TB, EPT> v;
+        v.load(ring.vec(u, q < nq ? q : nq - 1) + e);
+        if (q < nq) {
 #pragma unroll
-      for (int q = 0; q < NQ; ++q)
-        if (q < a.nq) acc[q] += (double)v[q] * wp;
+          for (int t = 0; t < EPT; ++t) sub[t] += v[t] * coef[q];
+        }
+      }
+      double wp[EPT];
+#pragma unroll
+      for (int t = 0; t < EPT; ++t) wp[t] = ws[t] - sub[t];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        Entries<TB, EPT> v;
+        v.load(ring.vec(u, q < nq ? q : nq - 1) + e);
+        if (q < nq) {
+#pragma unroll
+          for (int t = 0; t < EPT; ++t) acc[q] += v[t] * wp[t];
+        }
+      }
+    }
+    if (!ring.release(u)) {
+      ring.drain(u, a.err);
+      return;
     }
   }
-  const double r = gs_reduce_to_thread<NQ>(acc, scratch);
-  if (threadIdx.x < a.nq) a.part[(size_t)blockIdx.x * a.pstride + threadIdx.x] = r;
+  const double r = gs_block_reduce<NQ>(acc, reinterpret_cast<double*>(ring.stages));
+  if (threadIdx.x < nq) a.part[(size_t)blockIdx.x * a.pstride + threadIdx.x] = r;
 }
 
 // out = in - V (s h): pass 3, and the subtraction slices of the chained path ----
 template <typename TB, int NQ>
-__global__ void __launch_bounds__(kGB) k_gs_sub(Batch b, GsArgs<TB> a) {
+__global__ void __launch_bounds__(kGT) k_gs_sub(Batch b, GsArgs<TB> a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double coef[NQ];
   const Chunk ch = b.chunks[blockIdx.x];
   if (!case_live(b, ch.cs, a.need)) return;
   const CaseDev cs = b.cases[ch.cs];
   const size_t base = 4 * cs.cell_off + ch.begin;
-  __shared__ double coef[NQ];
-  __shared__ double scratch[8];
   coef_to_smem(a, ch.cs, b.ncases, coef, a.both != 0);
-  const TB* V = a.V + (size_t)a.q0 * a.vstride + base;
+  GsRing<TB> ring;
+  ring.init(smem, a, ch, base);
+  constexpr int EPT = GsRing<TB>::EPT;
+  constexpr int E = GsRing<TB>::E;
+  const int nq = a.nq;
   double nrm = 0.0;
 #pragma unroll 1
-  for (int s = 0; s < kGE / 4; ++s) {
-    const int e = 4 * (threadIdx.x + s * kGB);
-    if (e < ch.len) {
-      double sub[4] = {0.0, 0.0, 0.0, 0.0};
-      Raw4<TB> v[NQ];
+  for (int u = 0; u < ring.nsub; ++u) {
+    ring.wait(u);
+    const int e = threadIdx.x * EPT;
+    if (e < ring.len - u * E) {
+      const double* ws = ring.wvec(u) + e;
+      double sub[EPT];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) v[q].load(V + (size_t)(q < a.nq ? q : a.nq - 1) * a.vstride + e);
+      for (int t = 0; t < EPT; ++t) sub[t] = 0.0;
 #pragma unroll
       for (int q = 0; q < NQ; ++q) {
-        if (q < a.nq) {
+        Entries<TB, EPT> v;
+        v.load(ring.vec(u, q < nq ? q : nq - 1) + e);
+        if (q < nq) {
 #pragma unroll
-          for (int u = 0; u < 4; ++u) sub[u] += v[q][u] * coef[q];
+          for (int t = 0; t < EPT; ++t) sub[t] += v[t] * coef[q];
         }
       }
-      double w[4];
-      ldv(a.w + base + e, w);
+      const size_t g = base + (size_t)u * E + e;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        w[u] = w[u] - sub[u];
-        nrm += w[u] * w[u];
+      for (int t = 0; t < EPT; ++t) {
+        const double x = ws[t] - sub[t];
+        nrm += x * x;
+        if (a.wout != nullptr) a.wout[g + t] = x;
+        if (a.Vout != nullptr) a.Vout[g + t] = TB(x);
       }
-      if (a.wout != nullptr) stv(a.wout + base + e, w);
-      if (a.Vout != nullptr) stv(a.Vout + base + e, w);
+    }
+    if (!ring.release(u)) {
+      ring.drain(u, a.err);
+      return;
     }
   }
   if (a.part_norm != nullptr) {
     double v[1] = {nrm};
-    const double r = gs_reduce_to_thread<1>(v, scratch);
+    const double r = gs_block_reduce<1>(v, reinterpret_cast<double*>(ring.stages));
     if (threadIdx.x == 0) a.part_norm[blockIdx.x] = r;
   }
 }
@@ -306,14 +483,15 @@ __global__ void k_gs_close(Batch b, GsCloseArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int kSlice = 32;
 
-#define A2D_GS_DISPATCH(KERNEL)                                                            \
-  template <typename TB>                                                                   \
-  static void dispatch_##KERNEL(const Batch& b, const GsArgs<TB>& a, cudaStream_t s) {     \
-    if (!b.nchunks) return;                                                                \
-    if (a.nq <= 8) KERNEL<TB, 8><<<b.nchunks, kGB, 0, s>>>(b, a);                           \
-    else if (a.nq <= 16) KERNEL<TB, 16><<<b.nchunks, kGB, 0, s>>>(b, a);                    \
-    else if (a.nq <= 24) KERNEL<TB, 24><<<b.nchunks, kGB, 0, s>>>(b, a);                    \
-    else KERNEL<TB, 32><<<b.nchunks, kGB, 0, s>>>(b, a);                                    \
+#define A2D_GS_DISPATCH(KERNEL)                                                              \
+  template <typename TB>                                                                     \
+  static void dispatch_##KERNEL(const Batch& b, const GsArgs<TB>& a, cudaStream_t s) {       \
+    if (!b.nchunks) return;                                                                  \
+    const size_t smem = kGsHeader + (size_t)gs_stages<TB>(a.nq) * gs_stage_bytes<TB>(a.nq);  \
+    if (a.nq <= 8) KERNEL<TB, 8><<<b.nchunks, kGT, smem, s>>>(b, a);                          \
+    else if (a.nq <= 16) KERNEL<TB, 16><<<b.nchunks, kGT, smem, s>>>(b, a);                   \
+    else if (a.nq <= 24) KERNEL<TB, 24><<<b.nchunks, kGT, smem, s>>>(b, a);                   \
+    else KERNEL<TB, 32><<<b.nchunks, kGT, smem, s>>>(b, a);                                   \
   }
 A2D_GS_DISPATCH(k_gs_dots)
 A2D_GS_DISPATCH(k_gs_project)
@@ -393,5 +571,21 @@ void launch_gs_close(const Batch& b, const GsCloseArgs& a, cudaStream_t s) {
 A2D_GS_INST(double)
 A2D_GS_INST(float)
 #undef A2D_GS_INST
+
+cudaError_t gs_init() {
+  cudaError_t e = cudaSuccess;
+  const int bytes = (int)(kGsHeader + kGsSmemBudget);
+  auto set = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  };
+#define A2D_GS_ATTR(TB, NQ)                                            \
+  set(reinterpret_cast<const void*>(&k_gs_dots<TB, NQ>));              \
+  set(reinterpret_cast<const void*>(&k_gs_project<TB, NQ>));           \
+  set(reinterpret_cast<const void*>(&k_gs_sub<TB, NQ>));
+  A2D_GS_ATTR(float, 8) A2D_GS_ATTR(float, 16) A2D_GS_ATTR(float, 24) A2D_GS_ATTR(float, 32)
+  A2D_GS_ATTR(double, 8) A2D_GS_ATTR(double, 16) A2D_GS_ATTR(double, 24) A2D_GS_ATTR(double, 32)
+#undef A2D_GS_ATTR
+  return e;
+}
 
 }  // namespace a2d

@@ -28,6 +28,7 @@ struct GsArgs {
   double* wout = nullptr;         // subtraction result kept in FP64 (chained path)
   double* tmp = nullptr;          // scratch vector of the chained path (more than 32 vectors)
   double* part_norm = nullptr;    // per-chunk squared norm of the result
+  uint32_t* err = nullptr;        // set to 1 when a bulk-copy wait runs out of time
   uint32_t need = 0;
 };
 
@@ -60,5 +61,7 @@ template <typename TB> void launch_gs_project(const Batch& b, const GsArgs<TB>& 
 template <typename TB> void launch_gs_finish(const Batch& b, const GsArgs<TB>& a, cudaStream_t s);
 template <typename TB> void launch_gs_start(const Batch& b, const GsArgs<TB>& a, cudaStream_t s);
 void launch_gs_close(const Batch& b, const GsCloseArgs& a, cudaStream_t s);
+// raises the dynamic shared-memory limit of the streaming passes (host, once per device)
+cudaError_t gs_init();
 
 }  // namespace a2d

@@ -420,6 +420,7 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
     precond<TJ>(P, B, z, w, KR, s);
     // classical Gram-Schmidt run twice, three passes over the basis
     GsArgs<TB> g;
+    g.err = P->at<uint32_t>(P->o_cnt) + 1;
     g.w = w;
     g.V = V;
     g.vstride = vs;
@@ -652,6 +653,7 @@ int a2d_plan_bind(a2d_plan* P, void* workspace, size_t bytes, void* stream) {
   if (P->host_count == nullptr) A2D_CK(cudaMallocHost(&P->host_count, 2 * sizeof(int)));
   A2D_CK(cudaMemsetAsync(P->ws + P->o_cnt, 0, 8, s));
   A2D_CK(sweep_init());
+  A2D_CK(gs_init());
   k_reset<<<(P->ncases + 63) / 64, 64, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.cfl0);
   A2D_CK(cudaMemsetAsync(P->ws + P->o_circ_rk, 0, 8 * (size_t)P->ncases, s));
   A2D_CK(cudaGetLastError());
@@ -902,6 +904,7 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
         auto run = [&](auto* Vb) {
           using TB = std::remove_pointer_t<decltype(Vb)>;
           GsArgs<TB> g;
+          g.err = P->at<uint32_t>(P->o_cnt) + 1;
           g.w = P->vec(kW);
           g.V = Vb;
           g.vstride = vs;
