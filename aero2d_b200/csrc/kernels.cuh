@@ -1,11 +1,30 @@
 // Launcher declarations and argument blocks of the Euler-path kernels.
 #pragma once
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "batch.cuh"
 
 namespace a2d {
+
+// Storage type of the sweep factors (G, C, P, Q) for a Jacobian type: the
+// mixed-precision path keeps them in FP16 (they are products with the pivot
+// inverse, so their entries are O(1)); the pivot inverses stay in the Jacobian
+// type.  The factors only steer GMRES: the Newton residual stays FP64.
+template <typename TJ> struct FactorStore { using type = TJ; };
+template <> struct FactorStore<float> { using type = __half; };
+
+__device__ __forceinline__ double to_f64(float v) { return v; }
+__device__ __forceinline__ double to_f64(double v) { return v; }
+__device__ __forceinline__ double to_f64(__half v) { return (double)__half2float(v); }
+
+template <typename T> __device__ __forceinline__ T from_f64(double v) { return T(v); }
+// saturating: an entry beyond the FP16 range is stored as +-65504, never as inf
+template <> __device__ __forceinline__ __half from_f64<__half>(double v) {
+  const float f = (float)v;
+  return __float2half_rn(fminf(fmaxf(f, -65504.0f), 65504.0f));
+}
 
 template <typename VT>
 struct StencilArgs {

@@ -208,7 +208,7 @@ __device__ __forceinline__ void mul4_store(const double A[16], const double B[16
       double s = A[r * 4 + 0] * B[0 * 4 + c];
 #pragma unroll
       for (int k = 1; k < 4; ++k) s += A[r * 4 + k] * B[k * 4 + c];
-      out[q0 + (size_t)(r * 4 + c) * kLanes] = TF(s);
+      out[q0 + (size_t)(r * 4 + c) * kLanes] = from_f64<TF>(s);
     }
 }
 
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   const TJ* JIR = static_cast<const TJ*>(a.JIR);
   const TJ* JJL = static_cast<const TJ*>(a.JJL);
   const TJ* JJR = static_cast<const TJ*>(a.JJR);
-  TF* INV = static_cast<TF*>(a.INV);
+  TJ* INV = static_cast<TJ*>(a.INV);
   TF* CF = static_cast<TF*>(a.CF);
   TF* G = static_cast<TF*>(a.G);
   TF* P = static_cast<TF*>(a.P);
@@ -321,9 +321,9 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
       const size_t q = lbidx(cs.rows_nc, nc, grp.g, j, e, lane);
-      INV[q] = TF(inv[e]);
-      CF[q] = TF(cprev[e]);
-      G[q] = TF(D[e]);
+      INV[q] = TJ(inv[e]);
+      CF[q] = from_f64<TF>(cprev[e]);
+      G[q] = from_f64<TF>(D[e]);
     }
     // i-coupling of the sweeps, premultiplied: P = inv JIL(i), Q = inv JIR(i+1)
     load_block(JIL, cs.rows_nc, nc, grp.g, j, lane, T1);
@@ -347,6 +347,6 @@ void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s) {
 template void launch_face_jac<double>(const Batch&, const JacArgs&, cudaStream_t);
 template void launch_face_jac<float>(const Batch&, const JacArgs&, cudaStream_t);
 template void launch_factor<double, double>(const Batch&, const FactorArgs&, cudaStream_t);
-template void launch_factor<float, float>(const Batch&, const FactorArgs&, cudaStream_t);
+template void launch_factor<float, __half>(const Batch&, const FactorArgs&, cudaStream_t);
 
 }  // namespace a2d

@@ -73,6 +73,7 @@ struct a2d_plan {
   std::vector<long long> cp_off;
   long long C = 0, rows_nc = 0, rows_nc1 = 0, total_ni = 0;
   size_t tj = 8, tb = 8;   // bytes of face-Jacobian and basis storage entries
+  size_t tf = 8;           // bytes of the sweep factor entries (G, C, P, Q)
   // workspace layout (offsets)
   size_t o_cases = 0, o_tiles = 0, o_chunks = 0, o_groups = 0, o_cpoff = 0, o_live = 0, o_ctl = 0;
   size_t o_vec[kNumVec] = {};
@@ -160,10 +161,10 @@ static void layout(a2d_plan* P) {
   P->o_JJL = cv.take(P->tj * lb * P->rows_nc1);
   P->o_JJR = cv.take(P->tj * lb * P->rows_nc1);
   P->o_INV = cv.take(P->tj * lb * P->rows_nc);
-  P->o_CF = cv.take(P->tj * lb * P->rows_nc);
-  P->o_G = cv.take(P->tj * lb * P->rows_nc);
-  P->o_P = cv.take(P->tj * lb * P->rows_nc);
-  P->o_Q = cv.take(P->tj * lb * P->rows_nc);
+  P->o_CF = cv.take(P->tf * lb * P->rows_nc);
+  P->o_G = cv.take(P->tf * lb * P->rows_nc);
+  P->o_P = cv.take(P->tf * lb * P->rows_nc);
+  P->o_Q = cv.take(P->tf * lb * P->rows_nc);
   P->o_V = cv.take(P->tb * 4 * C * (size_t)(P->m + 1));
   P->o_H = cv.take(8 * (size_t)B * kMaxRestart * (kMaxRestart + 1));
   P->o_h1 = cv.take(8 * (size_t)B * kHStride);
@@ -329,7 +330,7 @@ static void precond_setup(a2d_plan* P, const Batch& B, uint32_t need, cudaStream
   ja.vortex = P->p.vortex_correction;
   ja.need = need;
   launch_face_jac<TJ>(B, ja, s);
-  launch_factor<TJ, TJ>(B, factor_args(P, need), s);
+  launch_factor<TJ, typename FactorStore<TJ>::type>(B, factor_args(P, need), s);
 }
 
 static StencilArgs<double> residual_args(a2d_plan* P) {
@@ -604,6 +605,7 @@ int a2d_plan_create(int ncases, const int* ni, const int* nc, const void* const*
   P->ncases = ncases;
   P->m = p.gmres_restart;
   P->tj = p.precision == A2D_MIXED ? 4 : 8;
+  P->tf = p.precision == A2D_MIXED ? 2 : 8;
   P->tb = p.precision == A2D_MIXED ? 4 : 8;
   build_tables(P, ni, nc, metrics, winf);
   layout(P);
@@ -950,7 +952,7 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
           else launch_face_jac<double>(B, ja, s);
         } else {
           const FactorArgs fa = factor_args(P, 0);
-          if (mixed) launch_factor<float, float>(B, fa, s);
+          if (mixed) launch_factor<float, __half>(B, fa, s);
           else launch_factor<double, double>(B, fa, s);
         }
         break;

@@ -14,7 +14,8 @@
 // One CTA of 128 threads per 32-line group: lane l = line, warp q = row of the
 // 4x4 blocks, so a warp reads one block entry of its 32 lines as 32
 // consecutive words of shared memory.  The blocks of every step (lane-blocked,
-// one contiguous 2 KB (FP32) / 4 KB (FP64) run per block) are streamed by the
+// one contiguous run per block: 1 KB for the FP16 factors of the mixed path,
+// 2 KB for its FP32 pivot inverses, 4 KB in FP64) are streamed by the
 // TMA engine through a ring of kStages stages, one mbarrier per stage, issued
 // kStages steps ahead by thread 0; the vector entries of the forward steps
 // come in the same ring by per-thread 8-byte cp.async.  The previous step's
@@ -31,27 +32,35 @@ constexpr int kSweepThreads = 128;
 constexpr int kBlockEntries = 16 * kLanes;   // one 4x4 block for the 32 lines of a group
 constexpr int kBackAhead = 8;                // register prefetch depth of d in the backward pass
 
-template <typename TF> struct SweepStages;
-template <> struct SweepStages<float> { static constexpr int value = 5; };
+// stages of the ring per Jacobian type (FP32: FP16 factors, 6 KB a stage)
+template <typename TI> struct SweepStages;
+template <> struct SweepStages<float> { static constexpr int value = 8; };
 template <> struct SweepStages<double> { static constexpr int value = 3; };
 
-template <typename TF>
+// TI: pivot inverses (the Jacobian type); TF: the other factors (FactorStore)
+template <typename TI>
 struct SweepSmem {
-  static constexpr int kS = SweepStages<TF>::value;
-  TF mat[kS][3][kBlockEntries];          // forward: (INV, G) or (P, Q, G); backward: C
+  using TF = typename FactorStore<TI>::type;
+  static constexpr int kS = SweepStages<TI>::value;
+  static constexpr uint32_t kBytesI = kBlockEntries * sizeof(TI);
+  static constexpr uint32_t kBytesF = kBlockEntries * sizeof(TF);
+  static constexpr uint32_t kMatBytes = (kBytesI + kBytesF > 3 * kBytesF) ? kBytesI + kBytesF : 3 * kBytesF;
+  // forward: (INV, G) or (P, Q, G); backward: C
+  alignas(128) unsigned char mat[kS][kMatBytes];
   double vec[kS][3][4][kLanes];          // forward: r or (e0, x'[i-1], x'[i+1]), [component][line]
   double xchg[2][4][kLanes];             // previous step's 4-vector of every line
   uint64_t full[kS];
   int abort[2];                          // wait failures, by step parity
 };
 
-template <typename TF, bool FIRST>
+template <typename TI, bool FIRST>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
+  using SM = SweepSmem<TI>;
+  using TF = typename SM::TF;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  SweepSmem<TF>& sm = *reinterpret_cast<SweepSmem<TF>*>(smem_raw);
-  constexpr int S = SweepSmem<TF>::kS;
-  constexpr int NM = FIRST ? 2 : 3;
-  constexpr uint32_t kBlockBytes = kBlockEntries * sizeof(TF);
+  SM& sm = *reinterpret_cast<SM*>(smem_raw);
+  constexpr int S = SM::kS;
+  constexpr uint32_t kBytesI = SM::kBytesI, kBytesF = SM::kBytesF;
   static_assert(S >= 2, "the vector copies are waited for one step ahead");
 
   const Group grp = b.groups[blockIdx.x];
@@ -68,9 +77,10 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   const int ip = (i + 1 == ni) ? 0 : i + 1;
   const size_t vb = 4 * (size_t)cs.cell_off;
   const size_t row_q = (size_t)q * nc * ni;   // component q of the case's vectors
-  const TF* fwd0 = static_cast<const TF*>(FIRST ? a.INV : a.P);
-  const TF* fwd1 = static_cast<const TF*>(FIRST ? a.G : a.Q);
-  const TF* fwd2 = static_cast<const TF*>(a.G);
+  const TI* INV = static_cast<const TI*>(a.INV);
+  const TF* Pm = static_cast<const TF*>(a.P);
+  const TF* Qm = static_cast<const TF*>(a.Q);
+  const TF* Gm = static_cast<const TF*>(a.G);
   const TF* CF = static_cast<const TF*>(a.CF);
   const size_t blk0 = lbidx(cs.rows_nc, nc, grp.g, 0, 0, 0);   // step j block at blk0 + j * kBlockEntries
   const int nsteps = 2 * nc;
@@ -88,16 +98,23 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
     if (t < nsteps) {
       const int s = t % S;
       if (tid == 0) {
+        unsigned char* m = sm.mat[s];
         if (t < nc) {
           const size_t o = blk0 + (size_t)t * kBlockEntries;
-          mbar_arrive_expect(&sm.full[s], NM * kBlockBytes);
-          bulk_load(sm.mat[s][0], fwd0 + o, kBlockBytes, &sm.full[s]);
-          bulk_load(sm.mat[s][1], fwd1 + o, kBlockBytes, &sm.full[s]);
-          if (!FIRST) bulk_load(sm.mat[s][2], fwd2 + o, kBlockBytes, &sm.full[s]);
+          if constexpr (FIRST) {
+            mbar_arrive_expect(&sm.full[s], kBytesI + kBytesF);
+            bulk_load(m, INV + o, kBytesI, &sm.full[s]);
+            bulk_load(m + kBytesI, Gm + o, kBytesF, &sm.full[s]);
+          } else {
+            mbar_arrive_expect(&sm.full[s], 3 * kBytesF);
+            bulk_load(m, Pm + o, kBytesF, &sm.full[s]);
+            bulk_load(m + kBytesF, Qm + o, kBytesF, &sm.full[s]);
+            bulk_load(m + 2 * kBytesF, Gm + o, kBytesF, &sm.full[s]);
+          }
         } else {
           const size_t o = blk0 + (size_t)(nsteps - 1 - t) * kBlockEntries;
-          mbar_arrive_expect(&sm.full[s], kBlockBytes);
-          bulk_load(sm.mat[s][0], CF + o, kBlockBytes, &sm.full[s]);
+          mbar_arrive_expect(&sm.full[s], kBytesF);
+          bulk_load(m, CF + o, kBytesF, &sm.full[s]);
         }
       }
       if (t < nc) {
@@ -132,32 +149,36 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   for (int t = 0; t < nc; ++t) {
     const int s = t % S;
     arrive(t);
-    const TF* M0 = sm.mat[s][0];
-    const TF* M1 = sm.mat[s][1];
+    const unsigned char* m = sm.mat[s];
     double e;
-    if (FIRST) {
+    const TF* Gs;
+    if constexpr (FIRST) {
+      const TI* M0 = reinterpret_cast<const TI*>(m);
+      Gs = reinterpret_cast<const TF*>(m + kBytesI);
       double r[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) r[c] = sm.vec[s][0][c][l];
-      e = (double)M0[(q * 4) * kLanes + l] * r[0];
+      e = to_f64(M0[(q * 4) * kLanes + l]) * r[0];
 #pragma unroll
-      for (int c = 1; c < 4; ++c) e += (double)M0[(q * 4 + c) * kLanes + l] * r[c];
+      for (int c = 1; c < 4; ++c) e += to_f64(M0[(q * 4 + c) * kLanes + l]) * r[c];
       if (a.e0 != nullptr && owner) a.e0[vb + row_q + (size_t)t * ni + i] = e;
     } else {
-      double s1 = (double)M0[(q * 4) * kLanes + l] * sm.vec[s][1][0][l];
-      double s2 = (double)M1[(q * 4) * kLanes + l] * sm.vec[s][2][0][l];
+      const TF* M0 = reinterpret_cast<const TF*>(m);
+      const TF* M1 = reinterpret_cast<const TF*>(m + kBytesF);
+      Gs = reinterpret_cast<const TF*>(m + 2 * kBytesF);
+      double s1 = to_f64(M0[(q * 4) * kLanes + l]) * sm.vec[s][1][0][l];
+      double s2 = to_f64(M1[(q * 4) * kLanes + l]) * sm.vec[s][2][0][l];
 #pragma unroll
       for (int c = 1; c < 4; ++c) {
-        s1 += (double)M0[(q * 4 + c) * kLanes + l] * sm.vec[s][1][c][l];
-        s2 += (double)M1[(q * 4 + c) * kLanes + l] * sm.vec[s][2][c][l];
+        s1 += to_f64(M0[(q * 4 + c) * kLanes + l]) * sm.vec[s][1][c][l];
+        s2 += to_f64(M1[(q * 4 + c) * kLanes + l]) * sm.vec[s][2][c][l];
       }
       e = sm.vec[s][0][q][l] + s1 - s2;
     }
-    const TF* Gs = FIRST ? M1 : sm.mat[s][2];
     const double* dp = &sm.xchg[(t + 1) & 1][0][0];
     double d = e;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) d += (double)Gs[(q * 4 + c) * kLanes + l] * dp[c * kLanes + l];
+    for (int c = 0; c < 4; ++c) d += to_f64(Gs[(q * 4 + c) * kLanes + l]) * dp[c * kLanes + l];
     sm.xchg[t & 1][q][l] = d;
     if (owner) x[(size_t)t * ni + i] = d;
     async_wait<S - 2>();
@@ -186,12 +207,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
           const int j = nc - 1 - bk;
           const int s = t % S;
           arrive(t);
-          const TF* C = sm.mat[s][0];
+          const TF* C = reinterpret_cast<const TF*>(sm.mat[s]);
           const double* xp = &sm.xchg[(t + 1) & 1][0][0];
           double acc = 0.0;
           if (bk > 0) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc += (double)C[(q * 4 + c) * kLanes + l] * xp[c * kLanes + l];
+            for (int c = 0; c < 4; ++c) acc += to_f64(C[(q * 4 + c) * kLanes + l]) * xp[c * kLanes + l];
           }
           const double xn = dbuf[u] - acc;
           sm.xchg[t & 1][q][l] = xn;
@@ -218,10 +239,10 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   }
 }
 
-template <typename TF, bool FIRST>
+template <typename TI, bool FIRST>
 void launch_sweep(const Batch& b, const SweepArgs& a, cudaStream_t s) {
   if (b.ngroups == 0) return;
-  k_sweep<TF, FIRST><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TF>), s>>>(b, a);
+  k_sweep<TI, FIRST><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TI>), s>>>(b, a);
 }
 
 cudaError_t sweep_init() {

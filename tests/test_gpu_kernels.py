@@ -121,7 +121,8 @@ def test_jvp_vs_complex_step(cuda, prec, tol):
 
 
 # ni = 64 fills two 32-line groups; ni = 80 leaves a partial third group.
-# Tolerances: FP64 factors 1e-10 relative; FP32-stored factors (mixed) 1e-4.
+# Tolerances: FP64 factors 1e-10 relative; mixed path (FP32 pivot inverses,
+# FP16 sweep factors) 5e-3.
 @pytest.mark.parametrize("ns,nj,sweeps,mixed", [(33, 25, 4, False), (41, 17, 1, False), (41, 17, 2, False),
                                                 (41, 17, 4, False), (41, 17, 4, True), (33, 25, 3, True)])
 def test_precond_vs_oracle(cuda, ns, nj, sweeps, mixed):
@@ -148,7 +149,7 @@ def test_precond_vs_oracle(cuda, ns, nj, sweeps, mixed):
     pl.set_vec(_lib.VEC_V, 0, torch.as_tensor(r))
     pl.precond_apply()
     x = pl.get_vec(_lib.VEC_JV, 0).cpu().numpy()
-    assert np.max(np.abs(x - xo)) / np.max(np.abs(xo)) < (1e-4 if mixed else 1e-10)
+    assert np.max(np.abs(x - xo)) / np.max(np.abs(xo)) < (5e-3 if mixed else 1e-10)
 
 
 def test_smoothing_vs_fft(cuda):
