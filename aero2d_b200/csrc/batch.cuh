@@ -173,6 +173,15 @@ __device__ __forceinline__ size_t lbidx(long long row0, int rows_per_line, int g
   return (((size_t)(row0 + (long long)g * rows_per_line + j)) * 16 + e) * kLanes + lane;
 }
 
+// index of entry (r, c) of row j of line (group g, lane) in the factor arrays of
+// the sweeps: the group's blocks of one row are one contiguous run, as in
+// lbidx, ordered [block row r][lane][column c], so that a thread holding block
+// row r of one line reads its four entries with one vector load
+__device__ __forceinline__ size_t fbidx(long long row0, int rows_per_line, int g, int j, int r, int c,
+                                        int lane) {
+  return ((((size_t)(row0 + (long long)g * rows_per_line + j)) * 4 + r) * kLanes + lane) * 4 + c;
+}
+
 __device__ __forceinline__ bool case_live(const Batch& b, int cs, uint32_t need) {
   return b.live == nullptr || (b.live[cs] & need) == need;
 }

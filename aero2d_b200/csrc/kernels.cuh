@@ -75,7 +75,10 @@ struct FactorArgs {
 // One line-Jacobi sweep x = M_line^-1 (r - off(xprev)), with the factors of
 // k_factor.  The first sweep (no previous iterate) computes e0 = inv r and may
 // keep it for the later sweeps, whose right-hand side is e0 + P xprev[i-1] -
-// Q xprev[i+1].
+// Q xprev[i+1].  All vectors are cell vectors [4][nc][ni]; r and the result of
+// the last sweep are FP64, the intermediate ones (e0, xprev, x of the other
+// sweeps) hold entries of the sweep's vector type (FP32 in the mixed path,
+// packed at the start of the buffer).
 struct SweepArgs {
   const double* r = nullptr;       // first sweep: right-hand side
   double* e0 = nullptr;            // first sweep: inv r written when set; later sweeps: read
@@ -105,9 +108,10 @@ void launch_face_jac(const Batch& b, const JacArgs& a, cudaStream_t s);
 template <typename TJ, typename TF>
 void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s);
 
-// one line-Jacobi sweep (sweep.cu); FIRST: the sweep without i-coupling
-template <typename TF, bool FIRST>
-void launch_sweep(const Batch& b, const SweepArgs& a, cudaStream_t s);
+// one line-Jacobi sweep (sweep.cu); FIRST: the sweep without i-coupling;
+// last: x is the FP64 result (else an intermediate vector)
+template <typename TI, bool FIRST>
+void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s);
 
 // raises the dynamic shared-memory limit of the sweep kernels (host, once per device)
 cudaError_t sweep_init();

@@ -198,9 +198,10 @@ __device__ __forceinline__ void load_block(const TJ* base, long long row0, int r
   for (int e = 0; e < 16; ++e) A[e] = (double)base[lbidx(row0, rows, g, j, e, lane)];
 }
 
-// out = A B (4x4, FP64), stored in TF at lane-blocked entries q0 + e * kLanes
+// out = A B (4x4, FP64), stored in TF in the sweep layout (fbidx)
 template <typename TF>
-__device__ __forceinline__ void mul4_store(const double A[16], const double B[16], TF* out, size_t q0) {
+__device__ __forceinline__ void mul4_store(const double A[16], const double B[16], TF* out, long long row0,
+                                           int rows, int g, int j, int lane) {
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -208,7 +209,7 @@ __device__ __forceinline__ void mul4_store(const double A[16], const double B[16
       double s = A[r * 4 + 0] * B[0 * 4 + c];
 #pragma unroll
       for (int k = 1; k < 4; ++k) s += A[r * 4 + k] * B[k * 4 + c];
-      out[q0 + (size_t)(r * 4 + c) * kLanes] = from_f64<TF>(s);
+      out[fbidx(row0, rows, g, j, r, c, lane)] = from_f64<TF>(s);
     }
 }
 
@@ -320,16 +321,16 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
       }
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
-      const size_t q = lbidx(cs.rows_nc, nc, grp.g, j, e, lane);
+      const size_t q = fbidx(cs.rows_nc, nc, grp.g, j, e >> 2, e & 3, lane);
       INV[q] = TJ(inv[e]);
       CF[q] = from_f64<TF>(cprev[e]);
       G[q] = from_f64<TF>(D[e]);
     }
     // i-coupling of the sweeps, premultiplied: P = inv JIL(i), Q = inv JIR(i+1)
     load_block(JIL, cs.rows_nc, nc, grp.g, j, lane, T1);
-    mul4_store(inv, T1, P, lbidx(cs.rows_nc, nc, grp.g, j, 0, lane));
+    mul4_store(inv, T1, P, cs.rows_nc, nc, grp.g, j, lane);
     load_block(JIR, cs.rows_nc, nc, gp, j, lp, T1);
-    mul4_store(inv, T1, Q, lbidx(cs.rows_nc, nc, grp.g, j, 0, lane));
+    mul4_store(inv, T1, Q, cs.rows_nc, nc, grp.g, j, lane);
   }
 }
 

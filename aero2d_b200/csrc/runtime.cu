@@ -310,11 +310,12 @@ static void precond(a2d_plan* P, const Batch& B, const double* rin, double* dst,
   a.r = rin;
   a.e0 = sweeps > 1 ? P->vec(kPE) : nullptr;
   a.x = sweeps > 1 ? bufs[0] : dst;
-  launch_sweep<TJ, true>(B, a, s);
+  launch_sweep<TJ, true>(B, a, sweeps == 1, s);
   for (int sw = 1; sw < sweeps; ++sw) {
+    const bool last = sw == sweeps - 1;
     a.xprev = a.x;
-    a.x = (sw == sweeps - 1) ? dst : bufs[sw & 1];
-    launch_sweep<TJ, false>(B, a, s);
+    a.x = last ? dst : bufs[sw & 1];
+    launch_sweep<TJ, false>(B, a, last, s);
   }
 }
 
@@ -885,8 +886,8 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
         a.e0 = P->vec(kPE);
         a.xprev = P->vec(kPB);
         a.x = P->vec(kPA);
-        if (mixed) launch_sweep<float, false>(B, a, s);
-        else launch_sweep<double, false>(B, a, s);
+        if (mixed) launch_sweep<float, false>(B, a, false, s);
+        else launch_sweep<double, false>(B, a, false, s);
         break;
       }
       case A2D_K_SWEEP_FIRST: {
@@ -894,8 +895,8 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
         a.r = P->vec(kZ);
         a.e0 = P->vec(kPE);
         a.x = P->vec(kPA);
-        if (mixed) launch_sweep<float, true>(B, a, s);
-        else launch_sweep<double, true>(B, a, s);
+        if (mixed) launch_sweep<float, true>(B, a, false, s);
+        else launch_sweep<double, true>(B, a, false, s);
         break;
       }
       case A2D_K_DOTS:

@@ -12,16 +12,23 @@
 // x'[i-1] + JIR(i+1) x'[i+1], the reference's sweep.
 //
 // One CTA of 128 threads per 32-line group: lane l = line, warp q = row of the
-// 4x4 blocks, so a warp reads one block entry of its 32 lines as 32
-// consecutive words of shared memory.  The blocks of every step (lane-blocked,
-// one contiguous run per block: 1 KB for the FP16 factors of the mixed path,
-// 2 KB for its FP32 pivot inverses, 4 KB in FP64) are streamed by the
-// TMA engine through a ring of kStages stages, one mbarrier per stage, issued
-// kStages steps ahead by thread 0; the vector entries of the forward steps
-// come in the same ring by per-thread 8-byte cp.async.  The previous step's
-// 4-vector passes between the four row warps through a two-slot exchange
-// buffer, with one CTA barrier per step.  d_j goes to x in HBM (mostly L2) and
-// comes back, register-prefetched, in the backward recurrence.
+// 4x4 blocks.  The blocks of every step are one contiguous run per factor
+// (fbidx: [row q][line][column c], so a thread's four entries are one vector
+// load and a warp reads 256 B in one go), streamed by the TMA engine through a
+// ring of kStages stages, one mbarrier per stage, issued kStages steps ahead by
+// thread 0; the vector entries of the forward steps come in the same ring by
+// per-thread cp.async, stored [line][component] so that a thread reads the
+// 4-vector of its line with one load.  The previous step's 4-vector passes
+// between the four row warps through a two-slot exchange buffer, with one CTA
+// barrier per step.  d_j goes to x and comes back, register-prefetched, in the
+// backward recurrence.
+//
+// Arithmetic and intermediate vectors are in the sweep's compute type: FP64
+// in the FP64 path; FP32 in the mixed path, whose factors are FP16 and pivot
+// inverses FP32 (a preconditioner only steers GMRES; the Newton residual and
+// the Krylov reductions stay FP64).
+#include <type_traits>
+
 #include "batch.cuh"
 #include "kernels.cuh"
 #include "tma.cuh"
@@ -32,31 +39,71 @@ constexpr int kSweepThreads = 128;
 constexpr int kBlockEntries = 16 * kLanes;   // one 4x4 block for the 32 lines of a group
 constexpr int kBackAhead = 8;                // register prefetch depth of d in the backward pass
 
-// stages of the ring per Jacobian type (FP32: FP16 factors, 6 KB a stage)
-template <typename TI> struct SweepStages;
-template <> struct SweepStages<float> { static constexpr int value = 8; };
-template <> struct SweepStages<double> { static constexpr int value = 3; };
+// TI: pivot inverses (the Jacobian type); TF: the other factors (FactorStore);
+// TC: arithmetic and intermediate vectors
+template <typename TI> struct SweepTypes;
+template <> struct SweepTypes<float> {
+  using TF = __half;
+  using TC = float;
+  static constexpr int kStages = 8;
+};
+template <> struct SweepTypes<double> {
+  using TF = double;
+  using TC = double;
+  static constexpr int kStages = 3;
+};
 
-// TI: pivot inverses (the Jacobian type); TF: the other factors (FactorStore)
 template <typename TI>
 struct SweepSmem {
-  using TF = typename FactorStore<TI>::type;
-  static constexpr int kS = SweepStages<TI>::value;
+  using TF = typename SweepTypes<TI>::TF;
+  using TC = typename SweepTypes<TI>::TC;
+  static constexpr int kS = SweepTypes<TI>::kStages;
   static constexpr uint32_t kBytesI = kBlockEntries * sizeof(TI);
   static constexpr uint32_t kBytesF = kBlockEntries * sizeof(TF);
   static constexpr uint32_t kMatBytes = (kBytesI + kBytesF > 3 * kBytesF) ? kBytesI + kBytesF : 3 * kBytesF;
-  // forward: (INV, G) or (P, Q, G); backward: C
-  alignas(128) unsigned char mat[kS][kMatBytes];
-  double vec[kS][3][4][kLanes];          // forward: r or (e0, x'[i-1], x'[i+1]), [component][line]
-  double xchg[2][4][kLanes];             // previous step's 4-vector of every line
+  // forward: r (FP64) or (e0, x'[i-1], x'[i+1]) in TC, each [line][component]
+  static constexpr uint32_t kVecBytes =
+      (3 * kLanes * 4 * sizeof(TC) > kLanes * 4 * sizeof(double)) ? 3 * kLanes * 4 * sizeof(TC)
+                                                                   : kLanes * 4 * sizeof(double);
+  alignas(128) unsigned char mat[kS][kMatBytes];   // forward: (INV, G) or (P, Q, G); backward: C
+  alignas(16) unsigned char vec[kS][kVecBytes];
+  alignas(16) TC xchg[2][kLanes][4];               // previous step's 4-vector of every line
   uint64_t full[kS];
-  int abort[2];                          // wait failures, by step parity
+  int abort[2];                                    // wait failures, by step parity
 };
 
-template <typename TI, bool FIRST>
+// the four entries of one block row of one line, converted to the compute type
+__device__ __forceinline__ void load4(const __half* p, float (&v)[4]) {
+  const uint2 raw = *reinterpret_cast<const uint2*>(p);
+  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void load4(const float* p, float (&v)[4]) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void load4(const double* p, float (&v)[4]) {
+  const double2 t0 = *reinterpret_cast<const double2*>(p);
+  const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = (float)t0.x; v[1] = (float)t0.y; v[2] = (float)t1.x; v[3] = (float)t1.y;
+}
+__device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
+  const double2 t0 = *reinterpret_cast<const double2*>(p);
+  const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
+}
+
+// asynchronous copy of one vector entry
+__device__ __forceinline__ void async_copy_entry(float* dst, const float* src) { async_copy4(dst, src); }
+__device__ __forceinline__ void async_copy_entry(double* dst, const double* src) { async_copy8(dst, src); }
+
+template <typename TI, bool FIRST, bool LAST>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   using SM = SweepSmem<TI>;
   using TF = typename SM::TF;
+  using TC = typename SM::TC;
+  using TX = typename std::conditional<LAST, double, TC>::type;   // type of x (and of d kept in it)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   SM& sm = *reinterpret_cast<SM*>(smem_raw);
   constexpr int S = SM::kS;
@@ -75,14 +122,17 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   const int i = grp.i0 + ll;
   const int im = (i == 0) ? ni - 1 : i - 1;
   const int ip = (i + 1 == ni) ? 0 : i + 1;
-  const size_t vb = 4 * (size_t)cs.cell_off;
-  const size_t row_q = (size_t)q * nc * ni;   // component q of the case's vectors
+  const size_t vq = 4 * (size_t)cs.cell_off + (size_t)q * nc * ni;   // component q of the case's vectors
   const TI* INV = static_cast<const TI*>(a.INV);
   const TF* Pm = static_cast<const TF*>(a.P);
   const TF* Qm = static_cast<const TF*>(a.Q);
   const TF* Gm = static_cast<const TF*>(a.G);
   const TF* CF = static_cast<const TF*>(a.CF);
+  const TC* e0v = reinterpret_cast<const TC*>(a.e0);
+  const TC* xpv = reinterpret_cast<const TC*>(a.xprev);
+  TX* x = reinterpret_cast<TX*>(a.x) + vq;
   const size_t blk0 = lbidx(cs.rows_nc, nc, grp.g, 0, 0, 0);   // step j block at blk0 + j * kBlockEntries
+  const int eo = (q * kLanes + l) * 4;                           // this thread's entries in a block
   const int nsteps = 2 * nc;
 
   if (tid == 0) {
@@ -91,7 +141,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
     mbar_init_fence();
     sm.abort[0] = sm.abort[1] = 0;
   }
-  sm.xchg[1][q][l] = 0.0;   // d_{-1} = 0
+  sm.xchg[1][l][q] = TC(0);   // d_{-1} = 0
+
+  // vector slot k of stage s, [line][component]; the first sweep's r slot is FP64
+  auto slot = [&](int s, int k) { return reinterpret_cast<TC*>(sm.vec[s]) + k * kLanes * 4; };
+  auto rslot = [&](int s) { return reinterpret_cast<double*>(sm.vec[s]); };
 
   // step t < nc: forward row j = t; t >= nc: backward row j = 2 nc - 1 - t
   auto issue = [&](int t) {
@@ -118,13 +172,13 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
         }
       }
       if (t < nc) {
-        const size_t row = vb + row_q + (size_t)t * ni;
-        if (FIRST) {
-          async_copy8(&sm.vec[s][0][q][l], a.r + row + i);
+        const size_t row = vq + (size_t)t * ni;
+        if constexpr (FIRST) {
+          async_copy8(rslot(s) + l * 4 + q, a.r + row + i);
         } else {
-          async_copy8(&sm.vec[s][0][q][l], a.e0 + row + i);
-          async_copy8(&sm.vec[s][1][q][l], a.xprev + row + im);
-          async_copy8(&sm.vec[s][2][q][l], a.xprev + row + ip);
+          async_copy_entry(slot(s, 0) + l * 4 + q, e0v + row + i);
+          async_copy_entry(slot(s, 1) + l * 4 + q, xpv + row + im);
+          async_copy_entry(slot(s, 2) + l * 4 + q, xpv + row + ip);
         }
       }
     }
@@ -142,7 +196,6 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   async_wait<S - 1>();
   __syncthreads();    // vector entries of step 0 visible to every warp
 
-  double* x = a.x + vb + row_q;
   int tstop = -1;     // step at which a wait ran out
   // ---- forward: d_j = e_j + G_j d_{j-1} ----
 #pragma unroll 1
@@ -150,37 +203,41 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
     const int s = t % S;
     arrive(t);
     const unsigned char* m = sm.mat[s];
-    double e;
+    TC e;
     const TF* Gs;
     if constexpr (FIRST) {
-      const TI* M0 = reinterpret_cast<const TI*>(m);
       Gs = reinterpret_cast<const TF*>(m + kBytesI);
-      double r[4];
+      TC iv[4], rv[4];
+      load4(reinterpret_cast<const TI*>(m) + eo, iv);
+      load4(rslot(s) + l * 4, rv);
+      e = iv[0] * rv[0];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) r[c] = sm.vec[s][0][c][l];
-      e = to_f64(M0[(q * 4) * kLanes + l]) * r[0];
-#pragma unroll
-      for (int c = 1; c < 4; ++c) e += to_f64(M0[(q * 4 + c) * kLanes + l]) * r[c];
-      if (a.e0 != nullptr && owner) a.e0[vb + row_q + (size_t)t * ni + i] = e;
+      for (int c = 1; c < 4; ++c) e += iv[c] * rv[c];
+      if (a.e0 != nullptr && owner) reinterpret_cast<TC*>(a.e0)[vq + (size_t)t * ni + i] = e;
     } else {
-      const TF* M0 = reinterpret_cast<const TF*>(m);
-      const TF* M1 = reinterpret_cast<const TF*>(m + kBytesF);
       Gs = reinterpret_cast<const TF*>(m + 2 * kBytesF);
-      double s1 = to_f64(M0[(q * 4) * kLanes + l]) * sm.vec[s][1][0][l];
-      double s2 = to_f64(M1[(q * 4) * kLanes + l]) * sm.vec[s][2][0][l];
+      TC pv[4], qv[4], xm[4], xp[4];
+      load4(reinterpret_cast<const TF*>(m) + eo, pv);
+      load4(reinterpret_cast<const TF*>(m + kBytesF) + eo, qv);
+      load4(slot(s, 1) + l * 4, xm);
+      load4(slot(s, 2) + l * 4, xp);
+      TC s1 = pv[0] * xm[0];
+      TC s2 = qv[0] * xp[0];
 #pragma unroll
       for (int c = 1; c < 4; ++c) {
-        s1 += to_f64(M0[(q * 4 + c) * kLanes + l]) * sm.vec[s][1][c][l];
-        s2 += to_f64(M1[(q * 4 + c) * kLanes + l]) * sm.vec[s][2][c][l];
+        s1 += pv[c] * xm[c];
+        s2 += qv[c] * xp[c];
       }
-      e = sm.vec[s][0][q][l] + s1 - s2;
+      e = slot(s, 0)[l * 4 + q] + s1 - s2;
     }
-    const double* dp = &sm.xchg[(t + 1) & 1][0][0];
-    double d = e;
+    TC gv[4], dp[4];
+    load4(Gs + eo, gv);
+    load4(&sm.xchg[(t + 1) & 1][l][0], dp);
+    TC d = e;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) d += to_f64(Gs[(q * 4 + c) * kLanes + l]) * dp[c * kLanes + l];
-    sm.xchg[t & 1][q][l] = d;
-    if (owner) x[(size_t)t * ni + i] = d;
+    for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
+    sm.xchg[t & 1][l][q] = d;
+    if (owner) x[(size_t)t * ni + i] = TX(d);
     async_wait<S - 2>();
     __syncthreads();
     if (sm.abort[t & 1]) {
@@ -191,11 +248,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   }
   // ---- backward: x_j = d_j - C_j x_{j+1} ----
   if (tstop < 0) {
-    double dbuf[kBackAhead];
+    TC dbuf[kBackAhead];
 #pragma unroll
     for (int u = 0; u < kBackAhead; ++u) {
       const int j = nc - 1 - u;
-      dbuf[u] = (j >= 0) ? x[(size_t)j * ni + i] : 0.0;
+      dbuf[u] = (j >= 0) ? TC(x[(size_t)j * ni + i]) : TC(0);
     }
 #pragma unroll 1
     for (int b0 = 0; b0 < nc && tstop < 0; b0 += kBackAhead) {
@@ -207,18 +264,20 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
           const int j = nc - 1 - bk;
           const int s = t % S;
           arrive(t);
-          const TF* C = reinterpret_cast<const TF*>(sm.mat[s]);
-          const double* xp = &sm.xchg[(t + 1) & 1][0][0];
-          double acc = 0.0;
+          TC acc = TC(0);
           if (bk > 0) {
+            TC cv[4], xn[4];
+            load4(reinterpret_cast<const TF*>(sm.mat[s]) + eo, cv);
+            load4(&sm.xchg[(t + 1) & 1][l][0], xn);
+            acc = cv[0] * xn[0];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc += to_f64(C[(q * 4 + c) * kLanes + l]) * xp[c * kLanes + l];
+            for (int c = 1; c < 4; ++c) acc += cv[c] * xn[c];
           }
-          const double xn = dbuf[u] - acc;
-          sm.xchg[t & 1][q][l] = xn;
-          if (owner) x[(size_t)j * ni + i] = xn;
+          const TC xv = dbuf[u] - acc;
+          sm.xchg[t & 1][l][q] = xv;
+          if (owner) x[(size_t)j * ni + i] = TX(xv);
           const int jn = j - kBackAhead;
-          if (jn >= 0) dbuf[u] = x[(size_t)jn * ni + i];
+          if (jn >= 0) dbuf[u] = TC(x[(size_t)jn * ni + i]);
           __syncthreads();
           if (sm.abort[t & 1]) tstop = t;
           else issue(t + S);
@@ -240,9 +299,10 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
 }
 
 template <typename TI, bool FIRST>
-void launch_sweep(const Batch& b, const SweepArgs& a, cudaStream_t s) {
+void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s) {
   if (b.ngroups == 0) return;
-  k_sweep<TI, FIRST><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TI>), s>>>(b, a);
+  if (last) k_sweep<TI, FIRST, true><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TI>), s>>>(b, a);
+  else k_sweep<TI, FIRST, false><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TI>), s>>>(b, a);
 }
 
 cudaError_t sweep_init() {
@@ -250,16 +310,18 @@ cudaError_t sweep_init() {
   auto set = [&](const void* f, size_t bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   };
-  set(reinterpret_cast<const void*>(&k_sweep<float, true>), sizeof(SweepSmem<float>));
-  set(reinterpret_cast<const void*>(&k_sweep<float, false>), sizeof(SweepSmem<float>));
-  set(reinterpret_cast<const void*>(&k_sweep<double, true>), sizeof(SweepSmem<double>));
-  set(reinterpret_cast<const void*>(&k_sweep<double, false>), sizeof(SweepSmem<double>));
+#define A2D_SWEEP_ATTR(TI, F, L) set(reinterpret_cast<const void*>(&k_sweep<TI, F, L>), sizeof(SweepSmem<TI>));
+  A2D_SWEEP_ATTR(float, true, true) A2D_SWEEP_ATTR(float, true, false)
+  A2D_SWEEP_ATTR(float, false, true) A2D_SWEEP_ATTR(float, false, false)
+  A2D_SWEEP_ATTR(double, true, true) A2D_SWEEP_ATTR(double, true, false)
+  A2D_SWEEP_ATTR(double, false, true) A2D_SWEEP_ATTR(double, false, false)
+#undef A2D_SWEEP_ATTR
   return e;
 }
 
-template void launch_sweep<float, true>(const Batch&, const SweepArgs&, cudaStream_t);
-template void launch_sweep<float, false>(const Batch&, const SweepArgs&, cudaStream_t);
-template void launch_sweep<double, true>(const Batch&, const SweepArgs&, cudaStream_t);
-template void launch_sweep<double, false>(const Batch&, const SweepArgs&, cudaStream_t);
+template void launch_sweep<float, true>(const Batch&, const SweepArgs&, bool, cudaStream_t);
+template void launch_sweep<float, false>(const Batch&, const SweepArgs&, bool, cudaStream_t);
+template void launch_sweep<double, true>(const Batch&, const SweepArgs&, bool, cudaStream_t);
+template void launch_sweep<double, false>(const Batch&, const SweepArgs&, bool, cudaStream_t);
 
 }  // namespace a2d

@@ -76,6 +76,11 @@ __device__ __forceinline__ void async_copy8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 
+// 4-byte asynchronous copy, global -> shared, by the calling thread
+__device__ __forceinline__ void async_copy4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
 __device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 
 // waits until at most N of the calling thread's committed groups are pending
