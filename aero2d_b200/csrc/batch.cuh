@@ -182,6 +182,13 @@ __device__ __forceinline__ size_t fbidx(long long row0, int rows_per_line, int g
   return ((((size_t)(row0 + (long long)g * rows_per_line + j)) * 4 + r) * kLanes + lane) * 4 + c;
 }
 
+// the same for the factors P, Q, G of the forward sweep (m = 0, 1, 2), kept
+// interleaved per row so that one copy brings all three blocks of a step
+__device__ __forceinline__ size_t fbidx3(long long row0, int rows_per_line, int g, int j, int m, int r, int c,
+                                         int lane) {
+  return (((((size_t)(row0 + (long long)g * rows_per_line + j)) * 3 + m) * 4 + r) * kLanes + lane) * 4 + c;
+}
+
 __device__ __forceinline__ bool case_live(const Batch& b, int cs, uint32_t need) {
   return b.live == nullptr || (b.live[cs] & need) == need;
 }

@@ -64,9 +64,8 @@ struct FactorArgs {
   const void* JJR = nullptr;
   void* INV = nullptr;             // inverse of the block-Thomas pivots [rows nc]
   void* CF = nullptr;              // upper factors c_j                 [rows nc]
-  void* G = nullptr;               // -inv_j A_j                         [rows nc]
-  void* P = nullptr;               // inv_j JIL(i)   (coupling to line i-1) [rows nc]
-  void* Q = nullptr;               // inv_j JIR(i+1) (coupling to line i+1) [rows nc]
+  void* PQG = nullptr;             // per row: P = inv_j JIL(i) (coupling to line i-1),
+                                   // Q = inv_j JIR(i+1) (to line i+1), G = -inv_j A_j  [rows nc]
   double* diag = nullptr;          // per-cell vol / dtau
   double cfl_base = 2.5;           // EulerSolver.cfl, which local_dt multiplies and step() divides out
   uint32_t need = 0;
@@ -84,10 +83,9 @@ struct SweepArgs {
   double* e0 = nullptr;            // first sweep: inv r written when set; later sweeps: read
   const double* xprev = nullptr;   // later sweeps: previous iterate (must not alias x)
   double* x = nullptr;             // result (the first sweep may write it over r)
+  double* dtmp = nullptr;          // last sweep: scratch for the forward values d_j
   const void* INV = nullptr;
-  const void* P = nullptr;
-  const void* Q = nullptr;
-  const void* G = nullptr;
+  const void* PQG = nullptr;       // P, Q, G blocks interleaved per row (fbidx3)
   const void* CF = nullptr;
   uint32_t* err = nullptr;         // set to 1 when a copy wait runs out of time
   uint32_t need = 0;

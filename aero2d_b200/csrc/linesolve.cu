@@ -198,10 +198,10 @@ __device__ __forceinline__ void load_block(const TJ* base, long long row0, int r
   for (int e = 0; e < 16; ++e) A[e] = (double)base[lbidx(row0, rows, g, j, e, lane)];
 }
 
-// out = A B (4x4, FP64), stored in TF in the sweep layout (fbidx)
+// block m of the interleaved P, Q, G rows = A B (4x4, FP64), stored in TF (fbidx3)
 template <typename TF>
 __device__ __forceinline__ void mul4_store(const double A[16], const double B[16], TF* out, long long row0,
-                                           int rows, int g, int j, int lane) {
+                                           int rows, int g, int j, int m, int lane) {
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -209,7 +209,7 @@ __device__ __forceinline__ void mul4_store(const double A[16], const double B[16
       double s = A[r * 4 + 0] * B[0 * 4 + c];
 #pragma unroll
       for (int k = 1; k < 4; ++k) s += A[r * 4 + k] * B[k * 4 + c];
-      out[fbidx(row0, rows, g, j, r, c, lane)] = from_f64<TF>(s);
+      out[fbidx3(row0, rows, g, j, m, r, c, lane)] = from_f64<TF>(s);
     }
 }
 
@@ -233,9 +233,7 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   const TJ* JJR = static_cast<const TJ*>(a.JJR);
   TJ* INV = static_cast<TJ*>(a.INV);
   TF* CF = static_cast<TF*>(a.CF);
-  TF* G = static_cast<TF*>(a.G);
-  TF* P = static_cast<TF*>(a.P);
-  TF* Q = static_cast<TF*>(a.Q);
+  TF* PQG = static_cast<TF*>(a.PQG);
   const double* U = a.U + 4 * cs.cell_off;
   const double cfl = a.ctl[grp.cs].cfl;
   double cprev[16];
@@ -324,13 +322,13 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
       const size_t q = fbidx(cs.rows_nc, nc, grp.g, j, e >> 2, e & 3, lane);
       INV[q] = TJ(inv[e]);
       CF[q] = from_f64<TF>(cprev[e]);
-      G[q] = from_f64<TF>(D[e]);
+      PQG[fbidx3(cs.rows_nc, nc, grp.g, j, 2, e >> 2, e & 3, lane)] = from_f64<TF>(D[e]);
     }
     // i-coupling of the sweeps, premultiplied: P = inv JIL(i), Q = inv JIR(i+1)
     load_block(JIL, cs.rows_nc, nc, grp.g, j, lane, T1);
-    mul4_store(inv, T1, P, cs.rows_nc, nc, grp.g, j, lane);
+    mul4_store(inv, T1, PQG, cs.rows_nc, nc, grp.g, j, 0, lane);
     load_block(JIR, cs.rows_nc, nc, gp, j, lp, T1);
-    mul4_store(inv, T1, Q, cs.rows_nc, nc, grp.g, j, lane);
+    mul4_store(inv, T1, PQG, cs.rows_nc, nc, grp.g, j, 1, lane);
   }
 }
 

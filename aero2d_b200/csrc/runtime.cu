@@ -55,7 +55,7 @@ static size_t metrics_total_bytes(int ni, int nc) {
   return metrics_float_offset(ni, nc) + metrics_floats(ni, nc) * 4;
 }
 
-enum VecSlot { kU = 0, kR, kVin, kJV, kDU, kB, kX0, kT, kRr, kZ, kW, kPA, kPB, kU0, kPE, kNumVec };
+enum VecSlot { kU = 0, kR, kVin, kJV, kDU, kB, kX0, kT, kRr, kZ, kW, kPA, kPB, kU0, kPE, kPD, kNumVec };
 
 }  // namespace a2d
 
@@ -77,7 +77,7 @@ struct a2d_plan {
   // workspace layout (offsets)
   size_t o_cases = 0, o_tiles = 0, o_chunks = 0, o_groups = 0, o_cpoff = 0, o_live = 0, o_ctl = 0;
   size_t o_vec[kNumVec] = {};
-  size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_G = 0, o_P = 0, o_Q = 0, o_V = 0;
+  size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_PQG = 0, o_V = 0;
   size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_lsq = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
   size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0;
   int pstride = 0;
@@ -162,9 +162,7 @@ static void layout(a2d_plan* P) {
   P->o_JJR = cv.take(P->tj * lb * P->rows_nc1);
   P->o_INV = cv.take(P->tj * lb * P->rows_nc);
   P->o_CF = cv.take(P->tf * lb * P->rows_nc);
-  P->o_G = cv.take(P->tf * lb * P->rows_nc);
-  P->o_P = cv.take(P->tf * lb * P->rows_nc);
-  P->o_Q = cv.take(P->tf * lb * P->rows_nc);
+  P->o_PQG = cv.take(3 * P->tf * lb * P->rows_nc);
   P->o_V = cv.take(P->tb * 4 * C * (size_t)(P->m + 1));
   P->o_H = cv.take(8 * (size_t)B * kMaxRestart * (kMaxRestart + 1));
   P->o_h1 = cv.take(8 * (size_t)B * kHStride);
@@ -272,9 +270,8 @@ namespace a2d {
 static SweepArgs sweep_args(const a2d_plan* P, uint32_t need) {
   SweepArgs a;
   a.INV = P->at<void>(P->o_INV);
-  a.P = P->at<void>(P->o_P);
-  a.Q = P->at<void>(P->o_Q);
-  a.G = P->at<void>(P->o_G);
+  a.PQG = P->at<void>(P->o_PQG);
+  a.dtmp = P->vec(kPD);
   a.CF = P->at<void>(P->o_CF);
   a.err = P->at<uint32_t>(P->o_cnt) + 1;
   a.need = need;
@@ -291,9 +288,7 @@ static FactorArgs factor_args(const a2d_plan* P, uint32_t need) {
   fa.JJR = P->at<void>(P->o_JJR);
   fa.INV = P->at<void>(P->o_INV);
   fa.CF = P->at<void>(P->o_CF);
-  fa.G = P->at<void>(P->o_G);
-  fa.P = P->at<void>(P->o_P);
-  fa.Q = P->at<void>(P->o_Q);
+  fa.PQG = P->at<void>(P->o_PQG);
   fa.diag = P->at<double>(P->o_diag);
   fa.cfl_base = P->p.cfl;
   fa.need = need;

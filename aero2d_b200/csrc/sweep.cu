@@ -20,8 +20,9 @@
 // per-thread cp.async, stored [line][component] so that a thread reads the
 // 4-vector of its line with one load.  The previous step's 4-vector passes
 // between the four row warps through a two-slot exchange buffer, with one CTA
-// barrier per step.  d_j goes to x and comes back, register-prefetched, in the
-// backward recurrence.
+// barrier per step.  d_j goes to x (the last sweep, whose x is FP64: to a
+// scratch vector) and comes back, register-prefetched, in the backward
+// recurrence.  The factors P, Q, G of a step are interleaved (fbidx3), one copy.
 //
 // Arithmetic and intermediate vectors are in the sweep's compute type: FP64
 // in the FP64 path; FP32 in the mixed path, whose factors are FP16 and pivot
@@ -124,13 +125,13 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   const int ip = (i + 1 == ni) ? 0 : i + 1;
   const size_t vq = 4 * (size_t)cs.cell_off + (size_t)q * nc * ni;   // component q of the case's vectors
   const TI* INV = static_cast<const TI*>(a.INV);
-  const TF* Pm = static_cast<const TF*>(a.P);
-  const TF* Qm = static_cast<const TF*>(a.Q);
-  const TF* Gm = static_cast<const TF*>(a.G);
+  const TF* PQG = static_cast<const TF*>(a.PQG);
   const TF* CF = static_cast<const TF*>(a.CF);
   const TC* e0v = reinterpret_cast<const TC*>(a.e0);
   const TC* xpv = reinterpret_cast<const TC*>(a.xprev);
   TX* x = reinterpret_cast<TX*>(a.x) + vq;
+  // d_j in the compute type: in x itself, or (last sweep, FP64 x) in the scratch
+  TC* dv = reinterpret_cast<TC*>(LAST ? a.dtmp : a.x) + vq;
   const size_t blk0 = lbidx(cs.rows_nc, nc, grp.g, 0, 0, 0);   // step j block at blk0 + j * kBlockEntries
   const int eo = (q * kLanes + l) * 4;                           // this thread's entries in a block
   const int nsteps = 2 * nc;
@@ -158,12 +159,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
           if constexpr (FIRST) {
             mbar_arrive_expect(&sm.full[s], kBytesI + kBytesF);
             bulk_load(m, INV + o, kBytesI, &sm.full[s]);
-            bulk_load(m + kBytesI, Gm + o, kBytesF, &sm.full[s]);
+            bulk_load(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, &sm.full[s]);
           } else {
+            // P, Q, G of the step: one contiguous 3-block run
             mbar_arrive_expect(&sm.full[s], 3 * kBytesF);
-            bulk_load(m, Pm + o, kBytesF, &sm.full[s]);
-            bulk_load(m + kBytesF, Qm + o, kBytesF, &sm.full[s]);
-            bulk_load(m + 2 * kBytesF, Gm + o, kBytesF, &sm.full[s]);
+            bulk_load(m, PQG + 3 * o, 3 * kBytesF, &sm.full[s]);
           }
         } else {
           const size_t o = blk0 + (size_t)(nsteps - 1 - t) * kBlockEntries;
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
     sm.xchg[t & 1][l][q] = d;
-    if (owner) x[(size_t)t * ni + i] = TX(d);
+    if (owner) dv[(size_t)t * ni + i] = d;
     async_wait<S - 2>();
     __syncthreads();
     if (sm.abort[t & 1]) {
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
 #pragma unroll
     for (int u = 0; u < kBackAhead; ++u) {
       const int j = nc - 1 - u;
-      dbuf[u] = (j >= 0) ? TC(x[(size_t)j * ni + i]) : TC(0);
+      dbuf[u] = (j >= 0) ? dv[(size_t)j * ni + i] : TC(0);
     }
 #pragma unroll 1
     for (int b0 = 0; b0 < nc && tstop < 0; b0 += kBackAhead) {
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
           sm.xchg[t & 1][l][q] = xv;
           if (owner) x[(size_t)j * ni + i] = TX(xv);
           const int jn = j - kBackAhead;
-          if (jn >= 0) dbuf[u] = TC(x[(size_t)jn * ni + i]);
+          if (jn >= 0) dbuf[u] = dv[(size_t)jn * ni + i];
           __syncthreads();
           if (sm.abort[t & 1]) tstop = t;
           else issue(t + S);
