@@ -182,14 +182,15 @@ def algorithmic_bytes(kernel: str, cells: int, restart: int, mixed: bool) -> flo
     cells); counts the matrix and vector words of the kernel's definition once."""
     f = 4 if mixed else 8
     h = 2 if mixed else 8   # sweep factors G, C, P, Q (FP16 in the mixed path)
+    v = 4 if mixed else 8   # intermediate vectors of the sweeps (FP32 in the mixed path)
     d = 8
     half = max(1, restart // 2)
     per_cell = {
         # coupled line sweep: e0, x_prev, P, Q, G, C, x (store); the d_j written by
         # the forward recurrence and read back by the backward one is not counted
-        "sweep": 4 * d + 4 * d + 4 * 16 * h + 4 * d,
+        "sweep": 4 * v + 4 * v + 4 * 16 * h + 4 * v,
         # first sweep: r, inv, G, C, e0 (store), x (store)
-        "sweep_first": 4 * d + 16 * f + 2 * 16 * h + 4 * d + 4 * d,
+        "sweep_first": 4 * d + 16 * f + 2 * 16 * h + 4 * v + 4 * v,
         # U, V, diag, z, face vectors (2 i-face + 2 j-face components)
         "jvp": 4 * d + 4 * f + d + 4 * d + 4 * f,
         # Gram-Schmidt pass 1: w, restart/2 basis vectors
