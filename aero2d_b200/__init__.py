@@ -5,7 +5,7 @@ Modules mirror the reference package layout for this path:
   grid      structured O-grid generator    (aero2d/grid.py)
   euler     residual, forces, RK4 + IRS    (aero2d/euler.py)
   implicit  Newton-Krylov solver           (aero2d/implicit.py)
-  service   continuous-batching request loop for polar sweeps
+  replicas  one process per GPU: case shards, job time, result gathering
 The numerics run in libaero2d_b200.so (hand-written sm_100a CUDA) through the
 C ABI of include/aero2d_b200.h.
 """

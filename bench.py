@@ -34,6 +34,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from aero2d_b200 import replicas  # noqa: E402  (host-only module: no torch or CUDA import)
+
 METRIC = "converged Euler cases/sec + p50/p99 latency, mixed vs plain FP64 on 1 B200 at |ΔCl|≤1e-4"
 GRID = dict(code="2412", n_side=129, nj=65, ds0=2e-3, radius=20.0)
 CASES = 64
@@ -245,7 +247,7 @@ def gpu_arm(args, rank: int, world: int, dist):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     B = args.cases
-    seed = SEED + rank
+    seed = replicas.rank_seed(SEED, rank)
     machs, alphas = draw_cases(seed, B)
     grid = make_grid()
 
@@ -276,12 +278,8 @@ def gpu_arm(args, rank: int, world: int, dist):
     converged = sum(int(r[3].sum()) for r in runs)
     kps, _ = plan.stats()
     launches = sum(r[5] * (kps + 1) + 2 for r in runs)
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        c = torch.tensor([float(converged)], dtype=torch.float64, device=dev)
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        elapsed_ms, converged = float(t.item()), int(c.item())
+    elapsed_ms, converged = replicas.job_time_and_count(elapsed_ms, converged, dist, dev)
+    converged = int(converged)
     step_ms, live = batch_solve.last_step_ms, batch_solve.last_live
     step_profile = {"ms_per_newton_step_by_live_cases": {
         f"{lo}-{hi}": round(float(step_ms[(live >= lo) & (live <= hi)].mean()), 3)
@@ -469,20 +467,12 @@ def main():
         profile_driver(args)
         return
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    rank, world, _ = replicas.env_rank_world()
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(reference_arm(args)))
         return
-    dist = None
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as td
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        dist = td
+    dist = replicas.init("nccl", timeout_s=300.0)
     try:
         out = gpu_arm(args, rank, world, dist)
         if rank == 0 and out is not None:
