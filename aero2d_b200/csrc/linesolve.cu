@@ -236,11 +236,10 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   TF* PQG = static_cast<TF*>(a.PQG);
   const double* U = a.U + 4 * cs.cell_off;
   const double cfl = a.ctl[grp.cs].cfl;
-  double cprev[16];
-#pragma unroll
-  for (int e = 0; e < 16; ++e) cprev[e] = 0.0;
-  for (int j = 0; j < nc; ++j) {
-    double D[16], T1[16];
+  const int k = nc / 2;   // twist row: the elimination from the wall and the one from the far field meet here
+  // D_j: the diagonal block of row j (face blocks + vol/dtau I); writes diag
+  auto assemble = [&](int j, double D[16]) {
+    double T1[16];
     load_block(JIL, cs.rows_nc, nc, gp, j, lp, D);
     load_block(JIR, cs.rows_nc, nc, grp.g, j, lane, T1);
 #pragma unroll
@@ -259,76 +258,118 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
       for (int e = 0; e < 16; ++e) D[e] = D[e] + T1[e];
     }
     // local pseudo-time step (aero2d/euler.py:289-296, aero2d/implicit.py:173-177)
-    {
-      const State4<double> W = cons_to_prim<double, double>(load_state<double>(U, g, j, i));
-      const double c = sqrt(kGamma * W.c[3] / W.c[0]);
-      const size_t N = (size_t)ni * nc;
-      const double* Si = g.Si;
-      const double* Sj = g.Sj;
-      const double s0 = 0.5 * (Si[(size_t)j * ni + i] + Si[(size_t)j * ni + ip]);
-      const double s1 = 0.5 * (Si[N + (size_t)j * ni + i] + Si[N + (size_t)j * ni + ip]);
-      const size_t NJ = (size_t)(nc + 1) * ni;
-      const double t0 = 0.5 * (Sj[(size_t)(j + 1) * ni + i] + Sj[(size_t)j * ni + i]);
-      const double t1 = 0.5 * (Sj[NJ + (size_t)(j + 1) * ni + i] + Sj[NJ + (size_t)j * ni + i]);
-      const double li = fabs(W.c[1] * s0 + W.c[2] * s1) + c * sqrt(s0 * s0 + s1 * s1);
-      const double lj = fabs(W.c[1] * t0 + W.c[2] * t1) + c * sqrt(t0 * t0 + t1 * t1);
-      const double vol = g.vol[(size_t)j * ni + i];
-      const double dt = a.cfl_base * vol / (li + lj);
-      const double dtl = dt / a.cfl_base * cfl;
-      const double dinv = 1.0 / dtl;
-      const double dg = vol * dinv;
-      a.diag[cs.cell_off + (size_t)j * ni + i] = dg;
-      D[0] += dg;
-      D[5] += dg;
-      D[10] += dg;
-      D[15] += dg;
-    }
-    // pivot block den = D - A c_prev with A = -JJL(j); inv = den^-1
-    double A[16];
-    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
+    const State4<double> W = cons_to_prim<double, double>(load_state<double>(U, g, j, i));
+    const double c = sqrt(kGamma * W.c[3] / W.c[0]);
+    const size_t N = (size_t)ni * nc;
+    const double* Si = g.Si;
+    const double* Sj = g.Sj;
+    const double s0 = 0.5 * (Si[(size_t)j * ni + i] + Si[(size_t)j * ni + ip]);
+    const double s1 = 0.5 * (Si[N + (size_t)j * ni + i] + Si[N + (size_t)j * ni + ip]);
+    const size_t NJ = (size_t)(nc + 1) * ni;
+    const double t0 = 0.5 * (Sj[(size_t)(j + 1) * ni + i] + Sj[(size_t)j * ni + i]);
+    const double t1 = 0.5 * (Sj[NJ + (size_t)(j + 1) * ni + i] + Sj[NJ + (size_t)j * ni + i]);
+    const double li = fabs(W.c[1] * s0 + W.c[2] * s1) + c * sqrt(s0 * s0 + s1 * s1);
+    const double lj = fabs(W.c[1] * t0 + W.c[2] * t1) + c * sqrt(t0 * t0 + t1 * t1);
+    const double vol = g.vol[(size_t)j * ni + i];
+    const double dt = a.cfl_base * vol / (li + lj);
+    const double dtl = dt / a.cfl_base * cfl;
+    const double dinv = 1.0 / dtl;
+    const double dg = vol * dinv;
+    a.diag[cs.cell_off + (size_t)j * ni + i] = dg;
+    D[0] += dg;
+    D[5] += dg;
+    D[10] += dg;
+    D[15] += dg;
+  };
+  // C = sgn A B (4x4)
+  auto mul = [](const double A[16], const double B[16], double C[16], double sgn) {
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        double s = A[r * 4 + 0] * cprev[0 * 4 + c];
+        double s = A[r * 4 + 0] * B[0 * 4 + c];
 #pragma unroll
-        for (int k = 1; k < 4; ++k) s += A[r * 4 + k] * cprev[k * 4 + c];
-        D[r * 4 + c] = D[r * 4 + c] + s;
+        for (int q = 1; q < 4; ++q) s += A[r * 4 + q] * B[q * 4 + c];
+        C[r * 4 + c] = sgn * s;
       }
-    double inv[16];
-    inv4(D, inv);
-    // G = inv * JJL(j) = -inv A: the forward recurrence becomes d_j = inv r_j + G d_{j-1}
+  };
+  // D += sgn A B
+  auto mul_add = [](const double A[16], const double B[16], double D[16], double sgn) {
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        double s = inv[r * 4 + 0] * A[0 * 4 + c];
+        double s = A[r * 4 + 0] * B[0 * 4 + c];
 #pragma unroll
-        for (int k = 1; k < 4; ++k) s += inv[r * 4 + k] * A[k * 4 + c];
-        D[r * 4 + c] = s;
+        for (int q = 1; q < 4; ++q) s += A[r * 4 + q] * B[q * 4 + c];
+        D[r * 4 + c] = D[r * 4 + c] + sgn * s;
       }
-    load_block(JJR, cs.rows_nc1, nc + 1, grp.g, j + 1, lane, T1);
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        double s = inv[r * 4 + 0] * T1[0 * 4 + c];
-#pragma unroll
-        for (int k = 1; k < 4; ++k) s += inv[r * 4 + k] * T1[k * 4 + c];
-        cprev[r * 4 + c] = s;
-      }
+  };
+  // row j's sweep factors: inv, G (the forward-recurrence coupling), C (the
+  // back-substitution coupling), and the i-couplings P = inv JIL(i), Q = inv JIR(i+1)
+  auto store_row = [&](int j, const double inv[16], const double Gm[16], const double Cm[16]) {
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
       const size_t q = fbidx(cs.rows_nc, nc, grp.g, j, e >> 2, e & 3, lane);
       INV[q] = TJ(inv[e]);
-      CF[q] = from_f64<TF>(cprev[e]);
-      PQG[fbidx3(cs.rows_nc, nc, grp.g, j, 2, e >> 2, e & 3, lane)] = from_f64<TF>(D[e]);
+      CF[q] = from_f64<TF>(Cm[e]);
+      PQG[fbidx3(cs.rows_nc, nc, grp.g, j, 2, e >> 2, e & 3, lane)] = from_f64<TF>(Gm[e]);
     }
-    // i-coupling of the sweeps, premultiplied: P = inv JIL(i), Q = inv JIR(i+1)
+    double T1[16];
     load_block(JIL, cs.rows_nc, nc, grp.g, j, lane, T1);
     mul4_store(inv, T1, PQG, cs.rows_nc, nc, grp.g, j, 0, lane);
     load_block(JIR, cs.rows_nc, nc, gp, j, lp, T1);
     mul4_store(inv, T1, PQG, cs.rows_nc, nc, grp.g, j, 1, lane);
+  };
+  // The line system is L_j x_{j-1} + D_j x_j + U_j x_{j+1} = r_j with L_j = -JJL(j),
+  // U_j = JJR(j+1) (aero2d/implicit.py:81-128).
+  // From the wall, rows 0 .. k-1: den_j = D_j - L_j c_{j-1}, c_j = den_j^-1 U_j,
+  // G_j = -den_j^-1 L_j; later d_j = inv_j r_j + G_j d_{j-1}, x_j = d_j - c_j x_{j+1}.
+  double cprev[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) cprev[e] = 0.0;
+  for (int j = 0; j < k; ++j) {
+    double D[16], A[16], inv[16], Gm[16], T1[16];
+    assemble(j, D);
+    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
+    mul_add(A, cprev, D, 1.0);
+    inv4(D, inv);
+    mul(inv, A, Gm, 1.0);
+    load_block(JJR, cs.rows_nc1, nc + 1, grp.g, j + 1, lane, T1);
+    mul(inv, T1, cprev, 1.0);
+    store_row(j, inv, Gm, cprev);
+  }
+  // From the far field, rows nc-1 .. k+1: den'_j = D_j - U_j c'_{j+1},
+  // c'_j = den'_j^-1 L_j, G'_j = -den'_j^-1 U_j; later d'_j = inv'_j r_j + G'_j d'_{j+1},
+  // x_j = d'_j - c'_j x_{j-1}.
+  double cnext[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) cnext[e] = 0.0;
+  for (int j = nc - 1; j > k; --j) {
+    double D[16], A[16], Um[16], inv[16], Gm[16];
+    assemble(j, D);
+    load_block(JJR, cs.rows_nc1, nc + 1, grp.g, j + 1, lane, Um);
+    mul_add(Um, cnext, D, -1.0);
+    inv4(D, inv);
+    mul(inv, Um, Gm, -1.0);
+    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
+    mul(inv, A, cnext, -1.0);
+    store_row(j, inv, Gm, cnext);
+  }
+  // Row k: den_k = D_k - L_k c_{k-1} - U_k c'_{k+1};
+  // x_k = inv_k r_k + G_k d_{k-1} + H_k d'_{k+1}, G_k = -inv_k L_k, H_k = -inv_k U_k
+  // (H is kept in the C slot of row k, which has no back substitution).
+  {
+    double D[16], A[16], Um[16], inv[16], Gm[16], Hm[16];
+    assemble(k, D);
+    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, k, lane, A);
+    load_block(JJR, cs.rows_nc1, nc + 1, grp.g, k + 1, lane, Um);
+    mul_add(A, cprev, D, 1.0);
+    mul_add(Um, cnext, D, -1.0);
+    inv4(D, inv);
+    mul(inv, A, Gm, 1.0);
+    mul(inv, Um, Hm, -1.0);
+    store_row(k, inv, Gm, Hm);
   }
 }
 
