@@ -430,31 +430,44 @@ __global__ void __launch_bounds__(kGB) k_gs_start(Batch b, GsArgs<TB> a) {
   if (threadIdx.x == 0) a.part_norm[blockIdx.x] = r;
 }
 
-// per-case reduction of the chunk partials, one block per case ----------------
-__global__ void k_gs_reduce(Batch b, GsReduceArgs a) {
+// sum over a case's chunks of one partial, by one warp: lane c takes chunks
+// c, c+32, ... in order, then a fixed butterfly; every lane gets the total
+__device__ __forceinline__ double warp_chunk_sum(const double* p, size_t stride, int nchunks) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int c = lane; c < nchunks; c += 32) s += p[(size_t)c * stride];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// per-case reduction of the chunk partials: one block per case, one warp per coefficient
+__global__ void __launch_bounds__(256) k_gs_reduce(Batch b, GsReduceArgs a) {
   const int cs_id = blockIdx.x;
   if (!case_live(b, cs_id, a.need)) return;
   const CaseDev cs = b.cases[cs_id];
   const int nred = a.nq + (a.wn0 != nullptr ? 1 : 0);
-  for (int q = threadIdx.x; q < nred; q += blockDim.x) {
-    double s = 0.0;
-    for (int c = 0; c < cs.nchunks; ++c) s += a.part[(size_t)(cs.chunk0 + c) * a.pstride + q];
-    if (q < a.nq) a.h[(size_t)cs_id * kHStride + q] = s * a.scale[(size_t)q * b.ncases + cs_id];
-    else a.wn0[cs_id] = sqrt(s);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = warp; q < nred; q += blockDim.x >> 5) {
+    const double s = warp_chunk_sum(a.part + (size_t)cs.chunk0 * a.pstride + q, a.pstride, cs.nchunks);
+    if (lane == 0) {
+      if (q < a.nq) a.h[(size_t)cs_id * kHStride + q] = s * a.scale[(size_t)q * b.ncases + cs_id];
+      else a.wn0[cs_id] = sqrt(s);
+    }
   }
 }
 
-// per-case close of an Arnoldi step (k >= 0) or of the start vector (k = -1) ----
-__global__ void k_gs_close(Batch b, GsCloseArgs a) {
-  const int cs_id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cs_id >= b.ncases) return;
+// per-case close of an Arnoldi step (k >= 0) or of the start vector (k = -1),
+// one warp per case ----
+__global__ void __launch_bounds__(32) k_gs_close(Batch b, GsCloseArgs a) {
+  const int cs_id = blockIdx.x;
   if ((a.live[cs_id] & a.need) != a.need) return;
   const CaseDev cs = b.cases[cs_id];
-  double s = 0.0;
-  for (int c = 0; c < cs.nchunks; ++c) s += a.part_norm[cs.chunk0 + c];
-  const double hn = sqrt(s);
+  const int lane = threadIdx.x;
+  const double hn = sqrt(warp_chunk_sum(a.part_norm + cs.chunk0, 1, cs.nchunks));
   CaseCtl& c = a.ctl[cs_id];
   if (a.k < 0) {
+    if (lane != 0) return;
     // _safe_normalize of the preconditioned residual: threshold eps
     const bool use = hn > DBL_EPSILON;
     const double beta = use ? hn : 0.0;
@@ -471,11 +484,13 @@ __global__ void k_gs_close(Batch b, GsCloseArgs a) {
   double* H = a.H + (size_t)cs_id * kMaxRestart * (kMaxRestart + 1) + (size_t)k * (kMaxRestart + 1);
   const double* h1 = a.h1 + (size_t)cs_id * kHStride;
   const double* h2 = a.h2 + (size_t)cs_id * kHStride;
-  for (int q = 0; q <= k; ++q) H[q] = h1[q] + h2[q];
-  H[k + 1] = use ? hn : 0.0;
-  a.scale[(size_t)(k + 1) * b.ncases + cs_id] = use ? 1.0 / hn : 0.0;
-  c.k_used = k + 1;
-  if (!use) a.live[cs_id] &= ~kLiveKrylov;
+  for (int q = lane; q <= k; q += 32) H[q] = h1[q] + h2[q];
+  if (lane == 0) {
+    H[k + 1] = use ? hn : 0.0;
+    a.scale[(size_t)(k + 1) * b.ncases + cs_id] = use ? 1.0 / hn : 0.0;
+    c.k_used = k + 1;
+    if (!use) a.live[cs_id] &= ~kLiveKrylov;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -557,10 +572,10 @@ void launch_gs_start(const Batch& b, const GsArgs<TB>& a, cudaStream_t s) {
   if (b.nchunks) k_gs_start<TB><<<b.nchunks, kGB, 0, s>>>(b, a);
 }
 void launch_gs_reduce(const Batch& b, const GsReduceArgs& a, cudaStream_t s) {
-  if (b.ncases) k_gs_reduce<<<b.ncases, 64, 0, s>>>(b, a);
+  if (b.ncases) k_gs_reduce<<<b.ncases, 256, 0, s>>>(b, a);
 }
 void launch_gs_close(const Batch& b, const GsCloseArgs& a, cudaStream_t s) {
-  k_gs_close<<<(b.ncases + 63) / 64, 64, 0, s>>>(b, a);
+  if (b.ncases) k_gs_close<<<b.ncases, 32, 0, s>>>(b, a);
 }
 
 #define A2D_GS_INST(TB)                                                                 \
