@@ -23,6 +23,7 @@
 // needed; w' is never stored, since pass 3 subtracts h1 + h2 from the
 // original w (equal to the two successive subtractions in exact arithmetic).
 #include <cfloat>
+#include <cuda_bf16.h>
 #include <type_traits>
 
 #include "batch.cuh"
@@ -94,6 +95,23 @@ __device__ __forceinline__ void stv(double* p, const double (&v)[4]) {
   *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
   *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
 }
+// one basis entry in FP64, and back in its storage precision
+__device__ __forceinline__ double entry_f64(double v) { return v; }
+__device__ __forceinline__ double entry_f64(float v) { return v; }
+__device__ __forceinline__ double entry_f64(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename TB> __device__ __forceinline__ TB to_basis(double x) { return TB(x); }
+template <> __device__ __forceinline__ __nv_bfloat16 to_basis<__nv_bfloat16>(double x) {
+  return __float2bfloat16_rn((float)x);
+}
+
+__device__ __forceinline__ void stv(__nv_bfloat16* p, const double (&v)[4]) {
+  __nv_bfloat162 lo = __floats2bfloat162_rn((float)v[0], (float)v[1]);
+  __nv_bfloat162 hi = __floats2bfloat162_rn((float)v[2], (float)v[3]);
+  uint2 raw;
+  raw.x = *reinterpret_cast<uint32_t*>(&lo);
+  raw.y = *reinterpret_cast<uint32_t*>(&hi);
+  *reinterpret_cast<uint2*>(p) = raw;
+}
 
 // ---------------------------------------------------------------------------
 // streaming passes.  A CTA of kGT threads owns one chunk and walks it in
@@ -108,7 +126,7 @@ __device__ __forceinline__ void stv(double* p, const double (&v)[4]) {
 // ---------------------------------------------------------------------------
 constexpr int kGT = 256;
 constexpr int kGsMaxStages = 8;
-constexpr size_t kGsSmemBudget = 72 * 1024;     // three CTAs per SM
+constexpr size_t kGsSmemBudget = 74 * 1024;     // three CTAs per SM
 constexpr int kGsHeader = 128;                  // mbarriers and abort flags before the stages
 
 template <typename TB> struct GsTile;
@@ -116,13 +134,15 @@ template <typename TB> struct GsTile;
 // rings; three CTAs per SM beat one CTA with more stages)
 template <> struct GsTile<float> { static constexpr int E = 512; };
 template <> struct GsTile<double> { static constexpr int E = 256; };
+template <> struct GsTile<__nv_bfloat16> { static constexpr int E = 1024; };
 
 template <typename TB>
 __host__ __device__ inline uint32_t gs_stage_bytes(int nq) {
   return (uint32_t)GsTile<TB>::E * (uint32_t)(nq * sizeof(TB) + 8);
 }
 static_assert(kGsSmemBudget >= (size_t)GsTile<float>::E * (32 * 4 + 8) &&
-                  kGsSmemBudget >= (size_t)GsTile<double>::E * (32 * 8 + 8),
+                  kGsSmemBudget >= (size_t)GsTile<double>::E * (32 * 8 + 8) &&
+                  kGsSmemBudget >= (size_t)GsTile<__nv_bfloat16>::E * (32 * 2 + 8),
               "one stage of a 32-vector slice must fit the shared-memory budget");
 
 template <typename TB>
@@ -163,6 +183,10 @@ template <> struct VecOf<double, 1> { using type = double; };
 template <> struct VecOf<double, 2> { using type = double2; };
 struct alignas(16) Double4x { double2 lo, hi; };
 template <> struct VecOf<double, 4> { using type = Double4x; };
+template <> struct VecOf<__nv_bfloat16, 1> { using type = __nv_bfloat16; };
+template <> struct VecOf<__nv_bfloat16, 2> { using type = __nv_bfloat162; };
+struct alignas(8) Bf16x4 { __nv_bfloat162 lo, hi; };
+template <> struct VecOf<__nv_bfloat16, 4> { using type = Bf16x4; };
 
 template <typename TB, int EPT>
 struct Entries {
@@ -171,7 +195,7 @@ struct Entries {
     using V = typename VecOf<TB, EPT>::type;
     *reinterpret_cast<V*>(v) = *reinterpret_cast<const V*>(p);
   }
-  __device__ __forceinline__ double operator[](int u) const { return (double)v[u]; }
+  __device__ __forceinline__ double operator[](int u) const { return entry_f64(v[u]); }
 };
 
 // the ring of one streaming pass over a chunk
@@ -390,7 +414,7 @@ __global__ void __launch_bounds__(kGT) k_gs_sub(Batch b, GsArgs<TB> a) {
         const double x = ws[t] - sub[t];
         nrm += x * x;
         if (a.wout != nullptr) a.wout[g + t] = x;
-        if (a.Vout != nullptr) a.Vout[g + t] = TB(x);
+        if (a.Vout != nullptr) a.Vout[g + t] = to_basis<TB>(x);
       }
     }
     if (!ring.release(u)) {
@@ -585,6 +609,7 @@ void launch_gs_close(const Batch& b, const GsCloseArgs& a, cudaStream_t s) {
   template void launch_gs_start<TB>(const Batch&, const GsArgs<TB>&, cudaStream_t);
 A2D_GS_INST(double)
 A2D_GS_INST(float)
+A2D_GS_INST(__nv_bfloat16)
 #undef A2D_GS_INST
 
 cudaError_t gs_init() {
@@ -599,6 +624,8 @@ cudaError_t gs_init() {
   set(reinterpret_cast<const void*>(&k_gs_sub<TB, NQ>));
   A2D_GS_ATTR(float, 8) A2D_GS_ATTR(float, 16) A2D_GS_ATTR(float, 24) A2D_GS_ATTR(float, 32)
   A2D_GS_ATTR(double, 8) A2D_GS_ATTR(double, 16) A2D_GS_ATTR(double, 24) A2D_GS_ATTR(double, 32)
+  A2D_GS_ATTR(__nv_bfloat16, 8) A2D_GS_ATTR(__nv_bfloat16, 16) A2D_GS_ATTR(__nv_bfloat16, 24)
+  A2D_GS_ATTR(__nv_bfloat16, 32)
 #undef A2D_GS_ATTR
   return e;
 }

@@ -9,6 +9,7 @@
 // squares, norms and the state update are FP64; the Krylov basis is stored as
 // TB (FP64, or FP32 in the mixed-precision mode).
 #include <cfloat>
+#include <cuda_bf16.h>
 
 #include "batch.cuh"
 #include "krylov.cuh"
@@ -112,6 +113,11 @@ __global__ void k_lstsq(int ncases, const uint32_t* live, CaseCtl* ctl, double* 
 }
 
 // dU = x0 + V y
+// one basis entry in FP64
+__device__ __forceinline__ double basis_f64(double v) { return v; }
+__device__ __forceinline__ double basis_f64(float v) { return v; }
+__device__ __forceinline__ double basis_f64(__nv_bfloat16 v) { return __bfloat162float(v); }
+
 template <typename TB>
 __global__ void __launch_bounds__(kVB) k_combine(Batch b, CombineArgs<TB> a) {
   const Chunk ch = b.chunks[blockIdx.x];
@@ -129,7 +135,7 @@ __global__ void __launch_bounds__(kVB) k_combine(Batch b, CombineArgs<TB> a) {
     const int e = threadIdx.x + s * kVB;
     if (e < ch.len) {
       double acc = 0.0;
-      for (int q = 0; q < k; ++q) acc += (double)a.V[(size_t)q * a.vstride + base + e] * ys[q];
+      for (int q = 0; q < k; ++q) acc += basis_f64(a.V[(size_t)q * a.vstride + base + e]) * ys[q];
       a.out[base + e] = a.x0[base + e] + acc;
     }
   }
@@ -357,5 +363,6 @@ void launch_mark_stepped(const Batch& b, const uint32_t* live, CaseCtl* ctl, cud
 
 template void launch_combine<double>(const Batch&, const CombineArgs<double>&, cudaStream_t);
 template void launch_combine<float>(const Batch&, const CombineArgs<float>&, cudaStream_t);
+template void launch_combine<__nv_bfloat16>(const Batch&, const CombineArgs<__nv_bfloat16>&, cudaStream_t);
 
 }  // namespace a2d

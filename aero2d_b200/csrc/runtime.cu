@@ -8,6 +8,7 @@
 // (rollback, freeze, SER CFL, convergence test, aero2d/implicit.py:216-244)
 // runs on the device, so the host synchronises once per step only to learn
 // whether any case is still live.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -54,6 +55,11 @@ struct Carve {
 static size_t metrics_total_bytes(int ni, int nc) {
   return metrics_float_offset(ni, nc) + metrics_floats(ni, nc) * 4;
 }
+
+// Krylov basis storage of the mixed path: BF16 (the basis is the raw,
+// unnormalised Arnoldi vectors with FP64 scales; Gram-Schmidt, the Hessenberg
+// matrix and the update are FP64)
+using Basis16 = __nv_bfloat16;
 
 enum VecSlot { kU = 0, kR, kVin, kJV, kDU, kB, kX0, kT, kRr, kZ, kW, kPA, kPB, kU0, kPE, kPD, kNumVec };
 
@@ -486,7 +492,7 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
 }
 
 static void newton_dispatch(a2d_plan* P, cudaStream_t s) {
-  if (P->p.precision == A2D_MIXED) newton_step_launches<float, float, float>(P, s);
+  if (P->p.precision == A2D_MIXED) newton_step_launches<float, float, Basis16>(P, s);
   else newton_step_launches<double, double, double>(P, s);
 }
 
@@ -602,7 +608,7 @@ int a2d_plan_create(int ncases, const int* ni, const int* nc, const void* const*
   P->m = p.gmres_restart;
   P->tj = p.precision == A2D_MIXED ? 4 : 8;
   P->tf = p.precision == A2D_MIXED ? 2 : 8;
-  P->tb = p.precision == A2D_MIXED ? 4 : 8;
+  P->tb = p.precision == A2D_MIXED ? sizeof(Basis16) : 8;
   build_tables(P, ni, nc, metrics, winf);
   layout(P);
   *out = P;
@@ -858,15 +864,15 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
     switch (which) {
       case A2D_K_JVP: {
         if (mixed) {
-          StencilArgs<float> a;
+          StencilArgs<Basis16> a;
           a.U = P->vec(kU);
-          a.V = P->at<float>(P->o_V);
+          a.V = P->at<Basis16>(P->o_V);
           a.diag = P->at<double>(P->o_diag);
           a.out = P->vec(kZ);
           a.lim_k = P->p.lim_k;
           a.order = P->p.order;
           a.vortex = P->p.vortex_correction;
-          launch_stencil<float, true, float>(B, a, s);
+          launch_stencil<float, true, Basis16>(B, a, s);
         } else {
           StencilArgs<double> a = residual_args(P);
           a.V = P->at<double>(P->o_V);
@@ -920,7 +926,7 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
           else if (which == A2D_K_PROJECT) launch_gs_project<TB>(B, g, s);
           else launch_gs_finish<TB>(B, g, s);
         };
-        if (mixed) run(P->at<float>(P->o_V));
+        if (mixed) run(P->at<Basis16>(P->o_V));
         else run(P->at<double>(P->o_V));
         break;
       }

@@ -5,6 +5,8 @@
 // product only defines the Krylov operator, while the FP64 residual on the
 // right-hand side fixes the converged solution, so FP32 operations a couple of
 // ulp off round-to-nearest are immaterial to the result.
+#include <cuda_bf16.h>
+
 #include "stencil_impl.cuh"
 
 namespace a2d {
@@ -12,5 +14,7 @@ namespace a2d {
 template void launch_stencil<float, false, double>(const Batch&, const StencilArgs<double>&, cudaStream_t);
 template void launch_stencil<float, true, double>(const Batch&, const StencilArgs<double>&, cudaStream_t);
 template void launch_stencil<float, true, float>(const Batch&, const StencilArgs<float>&, cudaStream_t);
+template void launch_stencil<float, true, __nv_bfloat16>(const Batch&, const StencilArgs<__nv_bfloat16>&,
+                                                         cudaStream_t);
 
 }  // namespace a2d
