@@ -185,6 +185,7 @@ def algorithmic_bytes(kernel: str, cells: int, restart: int, mixed: bool) -> flo
     f = 4 if mixed else 8
     h = 2 if mixed else 8   # sweep factors G, C, P, Q (FP16 in the mixed path)
     v = 4 if mixed else 8   # intermediate vectors of the sweeps (FP32 in the mixed path)
+    kb = 2 if mixed else 8  # Krylov basis entries (BF16 in the mixed path)
     d = 8
     half = max(1, restart // 2)
     per_cell = {
@@ -194,13 +195,13 @@ def algorithmic_bytes(kernel: str, cells: int, restart: int, mixed: bool) -> flo
         # first sweep: r, inv, G, C, e0 (store), x (store)
         "sweep_first": 4 * d + 16 * f + 2 * 16 * h + 4 * v + 4 * v,
         # U, V, diag, z, face vectors (2 i-face + 2 j-face components)
-        "jvp": 4 * d + 4 * f + d + 4 * d + 4 * f,
+        "jvp": 4 * d + 4 * kb + d + 4 * d + 4 * f,
         # Gram-Schmidt pass 1: w, restart/2 basis vectors
-        "dots": 4 * d + half * 4 * f,
+        "dots": 4 * d + half * 4 * kb,
         # pass 2: w, restart/2 basis vectors read once (kept on chip for the re-projection)
-        "project": 4 * d + half * 4 * f,
+        "project": 4 * d + half * 4 * kb,
         # pass 3: w, restart/2 basis vectors, the next basis vector written
-        "update": 4 * d + half * 4 * f + 4 * f,
+        "update": 4 * d + half * 4 * kb + 4 * kb,
     }[kernel]
     return float(per_cell) * cells
 
@@ -299,7 +300,7 @@ def gpu_arm(args, rank: int, world: int, dist):
                                f"seed {SEED}+rank, Newton-Krylov to residual drop {args.tol:g}",
                    "cases_per_gpu": B, "grid": "256x64 (ogrid naca4('2412',129), nj=65, ds0=2e-3, radius=20)",
                    "gmres_restart": args.restart, "jacobi_sweeps": 4, "max_newton_steps": args.max_iter,
-                   "precision": "mixed: FP64 residual/factorisation/Gram-Schmidt/update, FP32 JVP/face Jacobians/Krylov basis",
+                   "precision": "mixed: FP64 residual/factorisation/Gram-Schmidt/update; FP32 JVP, face Jacobians, sweep arithmetic; FP16 sweep factors; BF16 Krylov basis",
                    "l2": "working set ~2 GB per batch, larger than the 126 MB L2 (no flush needed)",
                    "parallelism": f"replicas x{world}, case sharding"},
         "converged_cases": converged,
