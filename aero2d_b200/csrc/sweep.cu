@@ -15,18 +15,21 @@
 // + JIR(i+1) x'[i+1]); eliminating from both ends halves the sequential depth
 // of a line from 2 nc to about nc dependent steps.
 //
-// One CTA of 256 threads per 32-line group: warps 0-3 run the wall half,
-// warps 4-7 the far-field half, in parallel; in each half lane l = line and
-// warp q = row of the 4x4 blocks.  Each half streams its rows' blocks (one
-// contiguous run per row: fbidx/fbidx3, a thread's block row is one vector
-// load) by TMA bulk copies through its own ring of kStages stages with one
-// mbarrier per stage, issued kStages steps ahead by the half's first thread;
-// the vector entries of the forward steps come in the same ring by per-thread
-// cp.async.  A line's 4-vector passes between the four row warps of a half
-// through a two-slot exchange buffer with one named barrier per step; the two
-// halves meet twice, around the twist row.  d_j goes to x (the last sweep,
-// whose x is FP64: to a scratch vector) and comes back, register-prefetched,
-// in the back substitution.
+// One CTA of nine warps per 32-line group, warp-specialised.  Warps 0-3 solve
+// the wall half and warps 4-7 the far-field half, in parallel (lane = line,
+// warp = row of the 4x4 blocks); warp 8 is the producer: for every step of each
+// half its lane 0 brings the step's blocks by TMA bulk copies (one contiguous
+// run per row: fbidx/fbidx3, a consumer's block row is one vector load) and
+// its lanes copy the step's vector entries of their line by cp.async, into a
+// ring of kStages stages per half with two mbarriers per stage: "full" (the
+// bulk-copy bytes plus one cp.async arrival per producer lane) and "empty" (one
+// arrival per consumer warp that is done with the stage).  The consumers only
+// compute: a line's 4-vector passes between the four row warps of a half
+// through a two-slot exchange buffer with one named barrier per step, and the
+// halves meet twice around the twist row.  d_j goes to x (the last sweep, whose
+// x is FP64: to a scratch vector) and comes back, register-prefetched, in the
+// back substitution.  Every wait is bounded; a wait that runs out records an
+// error and the CTA drains its copies in flight (bounded again) before exit.
 //
 // Arithmetic and intermediate vectors are in the sweep's compute type: FP64
 // in the FP64 path; FP32 in the mixed path, whose factors are FP16 and pivot
@@ -40,10 +43,12 @@
 
 namespace a2d {
 
-constexpr int kHalfThreads = 128;
-constexpr int kSweepThreads = 2 * kHalfThreads;
-constexpr int kBlockEntries = 16 * kLanes;   // one 4x4 block for the 32 lines of a group
-constexpr int kBackAhead = 8;                // register prefetch depth of d in the back substitution
+constexpr int kHalfThreads = 128;                       // consumer threads of one half
+constexpr int kConsumerThreads = 2 * kHalfThreads;
+constexpr int kProducerWarp = kConsumerThreads / 32;    // warp 8
+constexpr int kSweepThreads = kConsumerThreads + 32;
+constexpr int kBlockEntries = 16 * kLanes;              // one 4x4 block for the 32 lines of a group
+constexpr int kBackAhead = 8;                           // register prefetch depth of d in the back substitution
 
 // TI: pivot inverses (the Jacobian type); TF: the other factors (FactorStore);
 // TC: arithmetic and intermediate vectors
@@ -77,6 +82,7 @@ struct SweepSmem {
   alignas(16) TC xchg[2][2][kLanes][4];   // per half: the previous step's 4-vector of every line
   alignas(16) TC xk[kLanes][4];           // the twist row's solution
   uint64_t full[2][kS];
+  uint64_t empty[2][kS];
   int abort[2][2];                        // per half: wait failures, by step parity
   int failed[2];                          // per half: stopped early
 };
@@ -107,13 +113,17 @@ __device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
 __device__ __forceinline__ void async_copy_entry(float* dst, const float* src) { async_copy4(dst, src); }
 __device__ __forceinline__ void async_copy_entry(double* dst, const double* src) { async_copy8(dst, src); }
 
-// barrier of the 128 threads of one half (ids 1, 2; id 0 is __syncthreads)
+// barrier of the 128 consumer threads of one half (ids 1, 2) and of all 256
+// consumer threads (id 3); the producer warp takes part in none
 __device__ __forceinline__ void half_sync(int h) {
   asm volatile("bar.sync %0, %1;" ::"r"(1 + h), "r"(kHalfThreads) : "memory");
 }
+__device__ __forceinline__ void consumers_sync() {
+  asm volatile("bar.sync 3, %0;" ::"r"(kConsumerThreads) : "memory");
+}
 
 template <typename TI, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
+__global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a) {
   using SM = SweepSmem<TI>;
   using TF = typename SM::TF;
   using TC = typename SM::TC;
@@ -122,118 +132,169 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   SM& sm = *reinterpret_cast<SM*>(smem_raw);
   constexpr int S = SM::kS;
   constexpr uint32_t kBytesI = SM::kBytesI, kBytesF = SM::kBytesF;
-  static_assert(S >= 2, "the vector copies are waited for one step ahead");
+  constexpr uint32_t kOffG = FIRST ? kBytesI : 2 * kBytesF;   // G's block in a forward stage
+  constexpr uint32_t kOffH = kOffG + kBytesF;                // H's block in the twist stage
 
   const Group grp = b.groups[blockIdx.x];
   if (!case_live(b, grp.cs, a.need)) return;
   const int tid = threadIdx.x;
-  const int h = tid / kHalfThreads;           // 0: from the wall, 1: from the far field
-  const int ht = tid % kHalfThreads;          // thread within the half
-  const int l = ht & 31;                      // line within the group
-  const int q = ht >> 5;                      // row of the blocks owned by this warp
-  const bool owner = l < grp.n;               // lanes past the group's last line only compute
-  const int ll = owner ? l : grp.n - 1;       // and read a valid line
+  const int warp = tid >> 5, lane = tid & 31;
   const CaseDev cs = b.cases[grp.cs];
   const int ni = cs.g.ni, nc = cs.g.nc;
-  const int k = nc / 2;                       // twist row (as in k_factor)
-  const int nf = h == 0 ? k : nc - 1 - k;     // forward steps of this half
-  // step t of a half: t < nf forward; wall half t == k twist; then back substitution
-  const int nsteps = h == 0 ? 2 * k + 1 : 2 * nf;
-  auto row_of = [&](int t) {
+  const int k = nc / 2;                        // twist row (as in k_factor)
+  const int nf0 = k, nf1 = nc - 1 - k;         // forward steps of the wall / far-field half
+  const int ns0 = 2 * k + 1, ns1 = 2 * nf1;    // steps of each half
+  // step t of half h: forward rows first; the wall half's step k is the twist
+  // row; then the back substitution outward from the twist row
+  auto row_of = [&](int h, int t) {
     if (h == 0) return t <= k ? t : 2 * k - t;
-    return t < nf ? nc - 1 - t : k + 1 + (t - nf);
+    return t < nf1 ? nc - 1 - t : k + 1 + (t - nf1);
   };
-  const int i = grp.i0 + ll;
-  const int im = (i == 0) ? ni - 1 : i - 1;
-  const int ip = (i + 1 == ni) ? 0 : i + 1;
-  const size_t vq = 4 * (size_t)cs.cell_off + (size_t)q * nc * ni;   // component q of the case's vectors
-  const TI* INV = static_cast<const TI*>(a.INV);
-  const TF* PQG = static_cast<const TF*>(a.PQG);
-  const TF* CF = static_cast<const TF*>(a.CF);
-  const TC* e0v = reinterpret_cast<const TC*>(a.e0);
-  const TC* xpv = reinterpret_cast<const TC*>(a.xprev);
+  const size_t vbase = 4 * (size_t)cs.cell_off;
+  const size_t comp = (size_t)nc * ni;         // stride between the components of a case vector
+  const size_t blk0 = lbidx(cs.rows_nc, nc, grp.g, 0, 0, 0);   // row j's block at blk0 + j * kBlockEntries
+
+  if (tid == 0) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        mbar_init(&sm.full[h][s], 1 + 32);   // the bulk-copy arrival + one cp.async arrival per producer lane
+        mbar_init(&sm.empty[h][s], 4);       // one arrival per consumer warp of the half
+      }
+      sm.abort[h][0] = sm.abort[h][1] = 0;
+      sm.failed[h] = 0;
+    }
+    mbar_init_fence();
+  }
+  if (warp < kProducerWarp) {
+    const int h = warp >> 2, q = warp & 3;
+    sm.xchg[h][0][lane][q] = TC(0);
+    sm.xchg[h][1][lane][q] = TC(0);   // d_{-1} = d'_{nc} = 0
+  }
+  __syncthreads();
+
+  // ======================= producer warp =======================
+  if (warp == kProducerWarp) {
+    const int ll = lane < grp.n ? lane : grp.n - 1;
+    const int i = grp.i0 + ll;
+    const int im = (i == 0) ? ni - 1 : i - 1;
+    const int ip = (i + 1 == ni) ? 0 : i + 1;
+    const TI* INV = static_cast<const TI*>(a.INV);
+    const TF* PQG = static_cast<const TF*>(a.PQG);
+    const TF* CF = static_cast<const TF*>(a.CF);
+    const TC* e0v = reinterpret_cast<const TC*>(a.e0);
+    const TC* xpv = reinterpret_cast<const TC*>(a.xprev);
+    int issued[2] = {0, 0};
+    bool ok = true;
+    const int smax = ns0 > ns1 ? ns0 : ns1;
+#pragma unroll 1
+    for (int t = 0; t < smax && ok; ++t) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (!ok || t >= (h == 0 ? ns0 : ns1)) continue;
+        const int s = t % S;
+        if (t >= S && !mbar_wait(&sm.empty[h][s], ((t / S) - 1) & 1)) {
+          ok = false;
+          continue;
+        }
+        const int j = row_of(h, t);
+        const bool twist = h == 0 && t == k;
+        const bool fwd = twist || t < (h == 0 ? nf0 : nf1);
+        uint64_t* bar = &sm.full[h][s];
+        if (lane == 0) {
+          unsigned char* m = sm.mat[h][s];
+          const size_t o = blk0 + (size_t)j * kBlockEntries;
+          if (fwd) {
+            if constexpr (FIRST) {
+              mbar_arrive_expect(bar, kBytesI + (twist ? 2 : 1) * kBytesF);
+              bulk_load(m, INV + o, kBytesI, bar);
+              bulk_load(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, bar);
+              if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
+            } else {
+              mbar_arrive_expect(bar, (twist ? 4 : 3) * kBytesF);
+              bulk_load(m, PQG + 3 * o, 3 * kBytesF, bar);   // P, Q, G: one run
+              if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
+            }
+          } else {
+            mbar_arrive_expect(bar, kBytesF);
+            bulk_load(m, CF + o, kBytesF, bar);
+          }
+        }
+        if (fwd) {
+          const size_t row = vbase + (size_t)j * ni;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const size_t rc = row + c * comp;
+            if constexpr (FIRST) {
+              async_copy8(reinterpret_cast<double*>(sm.vec[h][s]) + lane * 4 + c, a.r + rc + i);
+            } else {
+              TC* v = reinterpret_cast<TC*>(sm.vec[h][s]) + lane * 4 + c;
+              async_copy_entry(v, e0v + rc + i);
+              async_copy_entry(v + kLanes * 4, xpv + rc + im);
+              async_copy_entry(v + 2 * kLanes * 4, xpv + rc + ip);
+            }
+          }
+        }
+        async_arrive(bar);   // lands once this lane's copies of the step have
+        issued[h] = t + 1;
+      }
+    }
+    if (!ok) {
+      // the consumers stopped: record it, and give the copies still in flight
+      // a bounded time to land before the CTA's shared memory goes away
+      if (lane == 0 && a.err != nullptr) atomicExch(a.err, 1u);
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h)
+        for (int u = issued[h] > S ? issued[h] - S : 0; u < issued[h]; ++u)
+          (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
+    }
+    return;
+  }
+
+  // ======================= consumers =======================
+  const int h = warp >> 2;                     // 0: from the wall, 1: from the far field
+  const int q = warp & 3;                      // row of the blocks owned by this warp
+  const int l = lane;                          // line within the group
+  const bool owner = l < grp.n;                // lanes past the group's last line only compute
+  const int i = grp.i0 + (owner ? l : grp.n - 1);
+  const int nf = h == 0 ? nf0 : nf1;
+  const int nsteps = h == 0 ? ns0 : ns1;
+  const size_t vq = vbase + (size_t)q * comp;  // component q of the case's vectors
   TX* x = reinterpret_cast<TX*>(a.x) + vq;
   // d_j in the compute type: in x itself, or (last sweep, FP64 x) in the scratch
   TC* dv = reinterpret_cast<TC*>(LAST ? a.dtmp : a.x) + vq;
-  const size_t blk0 = lbidx(cs.rows_nc, nc, grp.g, 0, 0, 0);   // row j's block at blk0 + j * kBlockEntries
-  const int eo = (q * kLanes + l) * 4;                           // this thread's entries in a block
-  uint64_t* full = sm.full[h];
+  const int eo = (q * kLanes + l) * 4;         // this thread's entries in a block
 
-  if (ht == 0) {
-#pragma unroll
-    for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
-    mbar_init_fence();
-    sm.abort[h][0] = sm.abort[h][1] = 0;
-    sm.failed[h] = 0;
-  }
-  sm.xchg[h][0][l][q] = TC(0);
-  sm.xchg[h][1][l][q] = TC(0);   // d_{-1} = d'_{nc} = 0
-
-  // vector slot k of stage s, [line][component]; the first sweep's r slot is FP64
-  auto slot = [&](int s, int kk) { return reinterpret_cast<TC*>(sm.vec[h][s]) + kk * kLanes * 4; };
-  auto rslot = [&](int s) { return reinterpret_cast<double*>(sm.vec[h][s]); };
-
-  auto issue = [&](int t) {
-    if (t < nsteps) {
-      const int s = t % S;
-      const int j = row_of(t);
-      const bool fwd = t < nf || (h == 0 && t == k);
-      if (ht == 0) {
-        unsigned char* m = sm.mat[h][s];
-        const size_t o = blk0 + (size_t)j * kBlockEntries;
-        if (fwd) {
-          const bool twist = h == 0 && t == k;
-          if constexpr (FIRST) {
-            mbar_arrive_expect(&full[s], kBytesI + (twist ? 2 : 1) * kBytesF);
-            bulk_load(m, INV + o, kBytesI, &full[s]);
-            bulk_load(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, &full[s]);
-            if (twist) bulk_load(m + kBytesI + kBytesF, CF + o, kBytesF, &full[s]);
-          } else {
-            mbar_arrive_expect(&full[s], (twist ? 4 : 3) * kBytesF);
-            bulk_load(m, PQG + 3 * o, 3 * kBytesF, &full[s]);   // P, Q, G: one run
-            if (twist) bulk_load(m + 3 * kBytesF, CF + o, kBytesF, &full[s]);
-          }
-        } else {
-          mbar_arrive_expect(&full[s], kBytesF);
-          bulk_load(m, CF + o, kBytesF, &full[s]);
-        }
-      }
-      if (fwd) {
-        const size_t row = vq + (size_t)j * ni;
-        if constexpr (FIRST) {
-          async_copy8(rslot(s) + l * 4 + q, a.r + row + i);
-        } else {
-          async_copy_entry(slot(s, 0) + l * 4 + q, e0v + row + i);
-          async_copy_entry(slot(s, 1) + l * 4 + q, xpv + row + im);
-          async_copy_entry(slot(s, 2) + l * 4 + q, xpv + row + ip);
-        }
-      }
-    }
-    async_commit();   // one group per step, empty ones included, keeps the group count regular
+  // waits for stage t of the half; a wait that runs out marks the step's
+  // parity slot, which every warp of the half reads after the step's barrier
+  auto wait_full = [&](int t) {
+    if (!mbar_wait(&sm.full[h][t % S], (t / S) & 1)) sm.abort[h][t & 1] = 1;
   };
-  // waits for the blocks of step t; a wait that runs out marks the step's parity
-  // slot, which every warp of the half reads after the step's barrier
-  auto arrive = [&](int t) {
-    if (!mbar_wait(&full[t % S], (t / S) & 1)) sm.abort[h][t & 1] = 1;
+  // this warp is done with stage t % S
+  auto release = [&](int t) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[h][t % S]);
   };
-  // e_j of step t (stage s) from the forward blocks
+  // e_j of stage s from the forward blocks and vector entries
   auto rhs = [&](int s, int j) -> TC {
     const unsigned char* m = sm.mat[h][s];
     TC e;
     if constexpr (FIRST) {
       TC iv[4], rv[4];
       load4(reinterpret_cast<const TI*>(m) + eo, iv);
-      load4(rslot(s) + l * 4, rv);
+      load4(reinterpret_cast<const double*>(sm.vec[h][s]) + l * 4, rv);
       e = iv[0] * rv[0];
 #pragma unroll
       for (int c = 1; c < 4; ++c) e += iv[c] * rv[c];
       if (a.e0 != nullptr && owner) reinterpret_cast<TC*>(a.e0)[vq + (size_t)j * ni + i] = e;
     } else {
+      const TC* vs = reinterpret_cast<const TC*>(sm.vec[h][s]);
       TC pv[4], qv[4], xm[4], xp[4];
       load4(reinterpret_cast<const TF*>(m) + eo, pv);
       load4(reinterpret_cast<const TF*>(m + kBytesF) + eo, qv);
-      load4(slot(s, 1) + l * 4, xm);
-      load4(slot(s, 2) + l * 4, xp);
+      load4(vs + kLanes * 4 + l * 4, xm);
+      load4(vs + 2 * kLanes * 4 + l * 4, xp);
       TC s1 = pv[0] * xm[0];
       TC s2 = qv[0] * xp[0];
 #pragma unroll
@@ -241,57 +302,48 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
         s1 += pv[c] * xm[c];
         s2 += qv[c] * xp[c];
       }
-      e = slot(s, 0)[l * 4 + q] + s1 - s2;
+      e = vs[l * 4 + q] + s1 - s2;
     }
     return e;
   };
-  constexpr uint32_t kOffG = FIRST ? kBytesI : 2 * kBytesF;   // G's block in a forward stage
-  constexpr uint32_t kOffH = kOffG + kBytesF;                // H's block in the twist stage
-
-  __syncthreads();    // barriers initialised, exchange slots cleared
-#pragma unroll 1
-  for (int t = 0; t < S; ++t) issue(t);
-  async_wait<S - 1>();
-  half_sync(h);       // vector entries of step 0 visible to every warp of the half
 
   int tstop = -1;     // step at which a wait ran out
   // ---- forward eliminations of both halves ----
 #pragma unroll 1
   for (int t = 0; t < nf; ++t) {
     const int s = t % S;
-    const int j = row_of(t);
-    arrive(t);
+    const int j = row_of(h, t);
+    wait_full(t);
     const TC e = rhs(s, j);
     TC gv[4], dp[4];
     load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
+    release(t);
     load4(&sm.xchg[h][(t + 1) & 1][l][0], dp);
     TC d = e;
 #pragma unroll
     for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
     sm.xchg[h][t & 1][l][q] = d;
     if (owner) dv[(size_t)j * ni + i] = d;
-    async_wait<S - 2>();
     half_sync(h);
     if (sm.abort[h][t & 1]) {
       tstop = t;
       break;
     }
-    issue(t + S);
   }
-  if (tstop >= 0 && ht == 0) sm.failed[h] = 1;
-  __syncthreads();    // (A) both forward eliminations done
-  const bool stop = sm.failed[0] || sm.failed[1];
+  if (tstop >= 0 && l == 0 && q == 0) sm.failed[h] = 1;
+  consumers_sync();   // (A) both forward eliminations done
   // ---- twist row k (wall half) ----
-  if (!stop && h == 0) {
+  if (!(sm.failed[0] || sm.failed[1]) && h == 0) {
     const int t = k;
     const int s = t % S;
-    arrive(t);
+    wait_full(t);
     const TC e = rhs(s, k);
     TC gv[4], hv[4], dm[4], dpl[4];
     load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
     load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffH) + eo, hv);
-    load4(&sm.xchg[0][(k + 1) & 1][l][0], dm);                               // d_{k-1}
-    if (nc - 1 - k > 0) load4(&sm.xchg[1][(nc - 1 - k + 1) & 1][l][0], dpl); // d'_{k+1}
+    release(t);
+    load4(&sm.xchg[0][(k + 1) & 1][l][0], dm);                        // d_{k-1}
+    if (nf1 > 0) load4(&sm.xchg[1][(nf1 + 1) & 1][l][0], dpl);        // d'_{k+1}
     else dpl[0] = dpl[1] = dpl[2] = dpl[3] = TC(0);
     TC xv = e;
 #pragma unroll
@@ -301,10 +353,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
     sm.xk[l][q] = xv;
     if (owner) x[(size_t)k * ni + i] = TX(xv);
     half_sync(h);
-    if (sm.abort[h][t & 1]) sm.failed[h] = 1;
-    else issue(t + S);
+    if (sm.abort[h][t & 1]) {
+      tstop = t;
+      if (l == 0 && q == 0) sm.failed[h] = 1;
+    }
   }
-  __syncthreads();    // (B) x_k visible to both halves
+  consumers_sync();   // (B) x_k visible to both halves
   // ---- back substitutions of both halves, outward from the twist row ----
   const int t0 = h == 0 ? k + 1 : nf;
   if (!(sm.failed[0] || sm.failed[1])) {
@@ -312,7 +366,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
 #pragma unroll
     for (int u = 0; u < kBackAhead; ++u) {
       const int t = t0 + u;
-      dbuf[u] = t < nsteps ? dv[(size_t)row_of(t) * ni + i] : TC(0);
+      dbuf[u] = t < nsteps ? dv[(size_t)row_of(h, t) * ni + i] : TC(0);
     }
 #pragma unroll 1
     for (int b0 = t0; b0 < nsteps && tstop < 0; b0 += kBackAhead) {
@@ -320,11 +374,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
       for (int u = 0; u < kBackAhead; ++u) {
         const int t = b0 + u;
         if (t < nsteps && tstop < 0) {
-          const int j = row_of(t);
+          const int j = row_of(h, t);
           const int s = t % S;
-          arrive(t);
+          wait_full(t);
           TC cv[4], xn[4];
           load4(reinterpret_cast<const TF*>(sm.mat[h][s]) + eo, cv);
+          release(t);
           load4(t == t0 ? &sm.xk[l][0] : &sm.xchg[h][(t + 1) & 1][l][0], xn);
           TC acc = cv[0] * xn[0];
 #pragma unroll
@@ -333,27 +388,19 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
           sm.xchg[h][t & 1][l][q] = xv;
           if (owner) x[(size_t)j * ni + i] = TX(xv);
           const int tn = t + kBackAhead;
-          if (tn < nsteps) dbuf[u] = dv[(size_t)row_of(tn) * ni + i];
+          if (tn < nsteps) dbuf[u] = dv[(size_t)row_of(h, tn) * ni + i];
           half_sync(h);
           if (sm.abort[h][t & 1]) tstop = t;
-          else issue(t + S);
         }
       }
     }
-  } else if (tstop < 0) {
-    // a half stopped: the copies this half issued beyond its last consumed
-    // step (the twist row for the wall half) are still to be drained
-    tstop = h == 0 ? k : nf;
   }
-  if (tstop >= 0) {
-    // a copy never completed: record it, and give the copies still in flight
-    // (issued for steps tstop .. tstop+S-1) a bounded time to land before exit
-    if (ht == 0) {
-      if (a.err != nullptr) atomicExch(a.err, 1u);
+  if (tstop >= 0 && l == 0 && q == 0) {
+    // a copy never landed: record it, and give the copies that may still be in
+    // flight for this half (issued for steps tstop .. tstop+S-1) a bounded time
+    if (a.err != nullptr) atomicExch(a.err, 1u);
 #pragma unroll 1
-      for (int u = tstop; u < tstop + S && u < nsteps; ++u) (void)mbar_wait(&full[u % S], (u / S) & 1);
-    }
-    async_wait<0>();
+    for (int u = tstop; u < tstop + S && u < nsteps; ++u) (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
   }
 }
 

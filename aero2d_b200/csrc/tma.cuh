@@ -83,6 +83,17 @@ __device__ __forceinline__ void async_copy4(void* dst, const void* src) {
 
 __device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 
+// one arrival on `bar`, triggered once every cp.async the calling thread issued
+// before it has completed (the arrival counts toward the expected count)
+__device__ __forceinline__ void async_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// one plain arrival (no transaction bytes)
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // waits until at most N of the calling thread's committed groups are pending
 template <int N>
 __device__ __forceinline__ void async_wait() {
