@@ -19,12 +19,12 @@
 // the wall half and warps 4-7 the far-field half, in parallel (lane = line,
 // warp = row of the 4x4 blocks); warp 8 is the producer: for every step of each
 // half its lane 0 brings the step's blocks by TMA bulk copies (one contiguous
-// run per row: fbidx/fbidx3, a consumer's block row is one vector load) and
-// its lanes copy the step's vector entries of their line by cp.async, into a
+// run per row: fbidx/fbidx3, a consumer's block row is one vector load) into a
 // ring of kStages stages per half with two mbarriers per stage: "full" (the
-// bulk-copy bytes plus one cp.async arrival per producer lane) and "empty" (one
-// arrival per consumer warp that is done with the stage).  The consumers only
-// compute: a line's 4-vector passes between the four row warps of a half
+// bulk-copy bytes) and "empty" (one arrival per consumer warp that is done with
+// the stage).  The consumers copy the vector entries of the forward steps into
+// the same stages by per-thread cp.async, kStages steps ahead, and compute: a
+// line's 4-vector passes between the four row warps of a half
 // through a two-slot exchange buffer with one named barrier per step, and the
 // halves meet twice around the twist row.  d_j goes to x (the last sweep, whose
 // x is FP64: to a scratch vector) and comes back, register-prefetched, in the
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     for (int h = 0; h < 2; ++h) {
 #pragma unroll
       for (int s = 0; s < S; ++s) {
-        mbar_init(&sm.full[h][s], 1 + 32);   // the bulk-copy arrival + one cp.async arrival per producer lane
+        mbar_init(&sm.full[h][s], 1);        // the producer's arrival with the bulk-copy bytes
         mbar_init(&sm.empty[h][s], 4);       // one arrival per consumer warp of the half
       }
       sm.abort[h][0] = sm.abort[h][1] = 0;
@@ -176,15 +176,9 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
 
   // ======================= producer warp =======================
   if (warp == kProducerWarp) {
-    const int ll = lane < grp.n ? lane : grp.n - 1;
-    const int i = grp.i0 + ll;
-    const int im = (i == 0) ? ni - 1 : i - 1;
-    const int ip = (i + 1 == ni) ? 0 : i + 1;
     const TI* INV = static_cast<const TI*>(a.INV);
     const TF* PQG = static_cast<const TF*>(a.PQG);
     const TF* CF = static_cast<const TF*>(a.CF);
-    const TC* e0v = reinterpret_cast<const TC*>(a.e0);
-    const TC* xpv = reinterpret_cast<const TC*>(a.xprev);
     int issued[2] = {0, 0};
     bool ok = true;
     const int smax = ns0 > ns1 ? ns0 : ns1;
@@ -221,22 +215,6 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
             bulk_load(m, CF + o, kBytesF, bar);
           }
         }
-        if (fwd) {
-          const size_t row = vbase + (size_t)j * ni;
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const size_t rc = row + c * comp;
-            if constexpr (FIRST) {
-              async_copy8(reinterpret_cast<double*>(sm.vec[h][s]) + lane * 4 + c, a.r + rc + i);
-            } else {
-              TC* v = reinterpret_cast<TC*>(sm.vec[h][s]) + lane * 4 + c;
-              async_copy_entry(v, e0v + rc + i);
-              async_copy_entry(v + kLanes * 4, xpv + rc + im);
-              async_copy_entry(v + 2 * kLanes * 4, xpv + rc + ip);
-            }
-          }
-        }
-        async_arrive(bar);   // lands once this lane's copies of the step have
         issued[h] = t + 1;
       }
     }
@@ -258,6 +236,8 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   const int l = lane;                          // line within the group
   const bool owner = l < grp.n;                // lanes past the group's last line only compute
   const int i = grp.i0 + (owner ? l : grp.n - 1);
+  const int im = (i == 0) ? ni - 1 : i - 1;
+  const int ip = (i + 1 == ni) ? 0 : i + 1;
   const int nf = h == 0 ? nf0 : nf1;
   const int nsteps = h == 0 ? ns0 : ns1;
   const size_t vq = vbase + (size_t)q * comp;  // component q of the case's vectors
@@ -265,6 +245,28 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   // d_j in the compute type: in x itself, or (last sweep, FP64 x) in the scratch
   TC* dv = reinterpret_cast<TC*>(LAST ? a.dtmp : a.x) + vq;
   const int eo = (q * kLanes + l) * 4;         // this thread's entries in a block
+  const TC* e0v = reinterpret_cast<const TC*>(a.e0) + vq;
+  const TC* xpv = reinterpret_cast<const TC*>(a.xprev) + vq;
+  const double* rv = a.r + vq;
+
+  // the vector entries of step t (forward steps and the twist row): each thread
+  // copies component q of its line into the stage; one cp.async group per step,
+  // empty ones included, keeps the group count regular
+  auto issue_vec = [&](int t) {
+    if (t < nf || (h == 0 && t == k)) {
+      const int s = t % S;
+      const size_t row = (size_t)row_of(h, t) * ni;
+      if constexpr (FIRST) {
+        async_copy8(reinterpret_cast<double*>(sm.vec[h][s]) + l * 4 + q, rv + row + i);
+      } else {
+        TC* v = reinterpret_cast<TC*>(sm.vec[h][s]) + l * 4 + q;
+        async_copy_entry(v, e0v + row + i);
+        async_copy_entry(v + kLanes * 4, xpv + row + im);
+        async_copy_entry(v + 2 * kLanes * 4, xpv + row + ip);
+      }
+    }
+    async_commit();
+  };
 
   // waits for stage t of the half; a wait that runs out marks the step's
   // parity slot, which every warp of the half reads after the step's barrier
@@ -307,6 +309,11 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     return e;
   };
 
+#pragma unroll 1
+  for (int t = 0; t < S; ++t) issue_vec(t);
+  async_wait<S - 1>();
+  half_sync(h);       // vector entries of step 0 visible to the half
+
   int tstop = -1;     // step at which a wait ran out
   // ---- forward eliminations of both halves ----
 #pragma unroll 1
@@ -324,11 +331,13 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
     sm.xchg[h][t & 1][l][q] = d;
     if (owner) dv[(size_t)j * ni + i] = d;
+    async_wait<S - 2>();   // this thread's entries of step t+1 landed; the barrier publishes them
     half_sync(h);
     if (sm.abort[h][t & 1]) {
       tstop = t;
       break;
     }
+    issue_vec(t + S);
   }
   if (tstop >= 0 && l == 0 && q == 0) sm.failed[h] = 1;
   consumers_sync();   // (A) both forward eliminations done
@@ -402,6 +411,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
 #pragma unroll 1
     for (int u = tstop; u < tstop + S && u < nsteps; ++u) (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
   }
+  if (tstop >= 0) async_wait<0>();   // this thread's own vector copies land before it exits
 }
 
 template <typename TI, bool FIRST>
