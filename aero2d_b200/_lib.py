@@ -102,6 +102,18 @@ SIGNATURES = {
     "a2d_set_circulation": (_I, [_P, C.POINTER(_D), _P]),
     "a2d_hllc_flux": (_I, [_I, _P, _P, _P, _P, _P]),
     "a2d_residual_norms_static": (_I, [_P, _I, _I, _I, _P, _P, _P, C.POINTER(Params), _P, _P, _P]),
+    "a2d_case_forces": (_I, [_P, C.POINTER(_D), C.POINTER(_D), _P]),
+    "a2d_case_restart": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_D), _I, _P]),
+    "a2d_case_retire": (_I, [_P, _I, C.POINTER(_I), _P]),
+    "a2d_service_create": (_I, [_I, _I, _P, _I, C.POINTER(Params), C.POINTER(_P)]),
+    "a2d_service_workspace_bytes": (_I, [_P, C.POINTER(_SZ)]),
+    "a2d_service_bind": (_I, [_P, _P, _SZ, _P]),
+    "a2d_service_submit": (_I, [_P, _I, C.POINTER(_D), _I, C.POINTER(C.c_longlong)]),
+    "a2d_service_step": (_I, [_P, C.POINTER(_I), _P]),
+    "a2d_service_poll": (_I, [_P, C.POINTER(C.c_longlong), _I, C.POINTER(_I)]),
+    "a2d_service_result": (_I, [_P, C.c_longlong, C.POINTER(_D), C.POINTER(_D), C.POINTER(_I), C.POINTER(_I)]),
+    "a2d_service_pending": (_I, [_P, C.POINTER(_I), C.POINTER(_I)]),
+    "a2d_service_destroy": (_I, [_P]),
 }
 
 _lib = None

@@ -90,7 +90,7 @@ struct CaseCtl {
   int commit;      // the last step was accepted
   int stepped;     // the case took the current step
   int nsteps;      // Newton steps taken
-  int pad;
+  int keep_r0;     // r0 was carried over from the previous point of a sweep
 };
 
 struct Batch {

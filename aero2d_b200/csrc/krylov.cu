@@ -278,7 +278,7 @@ __global__ void k_controller(Batch b, const double* tpart, CaseCtl* ctl, uint32_
   if (s.fails >= 5) s.frozen = 1;
   s.commit = bad ? 0 : 1;
   const double rnr = finite ? rn : NAN;
-  if (s.nsteps == 0) s.r0 = isfinite(rnr) ? fmax(rnr, 1e-30) : 1.0;
+  if (s.nsteps == 0 && !s.keep_r0) s.r0 = isfinite(rnr) ? fmax(rnr, 1e-30) : 1.0;
   const double den = isfinite(rnr) ? fmax(rnr, 1e-30) : s.r0;
   const double ser = p.cfl0 * (s.r0 / den);
   double cfl = fmin(fmax(ser, p.cfl0), p.cfl_max);

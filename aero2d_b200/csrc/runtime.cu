@@ -85,7 +85,7 @@ struct a2d_plan {
   size_t o_vec[kNumVec] = {};
   size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_PQG = 0, o_V = 0;
   size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_lsq = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
-  size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0;
+  size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0, o_idx = 0;
   int pstride = 0;
   size_t bytes = 0;
   char* ws = nullptr;
@@ -188,6 +188,7 @@ static void layout(a2d_plan* P) {
   P->o_hrn = cv.take(8 * (size_t)B * P->p.max_iter);
   P->o_hcl = cv.take(8 * (size_t)B * P->p.max_iter);
   P->o_cnt = cv.take(8);   // [0] live-case count, [1] sweep copy-wait failure flag
+  P->o_idx = cv.take(sizeof(int) * (size_t)B);   // case index lists of a2d_case_restart / _retire
   P->bytes = cv.off + 256;
 }
 
@@ -218,6 +219,45 @@ __global__ void k_reset(int ncases, CaseCtl* ctl, uint32_t* live, double cfl0) {
   c.omega = 1.0;
   ctl[k] = c;
   live[k] = kLiveNewton;
+}
+
+// restarts the listed cases (one block each) with the freestream now in their
+// table entry: U := freestream and Newton state as k_reset; with keep, U stays
+// (the previous point's solution) and so does r0, the residual reference of
+// the sweep's first (cold) point, so that the tolerance keeps its absolute
+// level and the SER CFL starts from the converged state's small residual
+__global__ void k_restart_cases(Batch b, const int* idx, int keep, double* U, CaseCtl* ctl, uint32_t* live,
+                                double cfl0) {
+  const int k = idx[blockIdx.x];
+  const CaseDev cs = b.cases[k];
+  if (!keep) {
+    const double rho = cs.winf[0], u = cs.winf[1], v = cs.winf[2], p = cs.winf[3];
+    const double Uc[4] = {rho, rho * u, rho * v, p / kGm1 + 0.5 * rho * (u * u + v * v)};
+    const long long n = (long long)cs.g.ni * cs.g.nc;
+    double* Uk = U + 4 * cs.cell_off;
+    for (long long c = threadIdx.x; c < n; c += blockDim.x) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) Uk[q * n + c] = Uc[q];
+    }
+  }
+  if (threadIdx.x == 0) {
+    const double r0 = ctl[k].r0;
+    const bool carry = keep && ctl[k].nsteps > 0 && isfinite(r0) && r0 > 0.0;
+    CaseCtl c{};
+    c.cfl = cfl0;
+    c.rn = NAN;
+    c.lastrn = NAN;
+    c.r0 = carry ? r0 : 1.0;
+    c.keep_r0 = carry ? 1 : 0;
+    c.omega = 1.0;
+    ctl[k] = c;
+    live[k] = kLiveNewton;
+  }
+}
+
+__global__ void k_retire_cases(const int* idx, int n, uint32_t* live) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) live[idx[q]] = 0;
 }
 
 __global__ void k_count(int ncases, const CaseCtl* ctl, const uint32_t* live, int retire, int* out) {
@@ -716,6 +756,55 @@ int a2d_reset(a2d_plan* P, void* stream) {
                                                                                 P->p.cfl0);
   A2D_CK(cudaGetLastError());
   P->steps_taken = 0;
+  return A2D_OK;
+}
+
+int a2d_case_restart(a2d_plan* P, int n, const int* cases, const double* winf, int keep_state, void* stream) {
+  A2D_BOUND(P);
+  if (n < 0 || n > P->ncases || (n > 0 && (cases == nullptr || winf == nullptr)))
+    return fail(A2D_ERR_ARG, "case_restart: bad arguments");
+  if (n == 0) return A2D_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (int q = 0; q < n; ++q) {
+    const int k = cases[q];
+    if (k < 0 || k >= P->ncases) return fail(A2D_ERR_ARG, "case_restart: case index out of range");
+    for (int c = 0; c < 4; ++c) P->cases[k].winf[c] = winf[4 * q + c];
+  }
+  // the per-case table and the index list; pageable sources are staged before the call returns
+  A2D_CK(cudaMemcpyAsync(P->ws + P->o_cases, P->cases.data(), sizeof(CaseDev) * P->ncases,
+                         cudaMemcpyHostToDevice, s));
+  A2D_CK(cudaMemcpyAsync(P->at<int>(P->o_idx), cases, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  k_restart_cases<<<n, 256, 0, s>>>(P->batch, P->at<int>(P->o_idx), keep_state, P->vec(kU), P->ctl(), P->live(),
+                                    P->p.cfl0);
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_case_forces(a2d_plan* P, double* coef, double* cp, void* stream) {
+  A2D_BOUND(P);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Batch B = P->batch;
+  B.live = nullptr;
+  launch_forces(B, P->vec(kU), P->at<double>(P->o_coef), P->at<double>(P->o_cp), P->at<long long>(P->o_cpoff),
+                nullptr, nullptr, 0, s);
+  if (coef != nullptr)
+    A2D_CK(cudaMemcpyAsync(coef, P->at<double>(P->o_coef), 8 * 3 * (size_t)P->ncases, cudaMemcpyDeviceToHost, s));
+  if (cp != nullptr)
+    A2D_CK(cudaMemcpyAsync(cp, P->at<double>(P->o_cp), 8 * (size_t)P->total_ni, cudaMemcpyDeviceToHost, s));
+  A2D_CK(cudaStreamSynchronize(s));
+  return A2D_OK;
+}
+
+int a2d_case_retire(a2d_plan* P, int n, const int* cases, void* stream) {
+  A2D_BOUND(P);
+  if (n < 0 || n > P->ncases || (n > 0 && cases == nullptr)) return fail(A2D_ERR_ARG, "case_retire: bad arguments");
+  if (n == 0) return A2D_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (int q = 0; q < n; ++q)
+    if (cases[q] < 0 || cases[q] >= P->ncases) return fail(A2D_ERR_ARG, "case_retire: case index out of range");
+  A2D_CK(cudaMemcpyAsync(P->at<int>(P->o_idx), cases, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  k_retire_cases<<<(n + 63) / 64, 64, 0, s>>>(P->at<int>(P->o_idx), n, P->live());
+  A2D_CK(cudaGetLastError());
   return A2D_OK;
 }
 

@@ -127,6 +127,46 @@ int a2d_case_status(const a2d_plan* plan, int* nsteps, int* done, int* frozen, d
  * step failed), step length omega, CFL of the next step, r0, circulation, ||M(b - A x0)||,
  * Arnoldi vectors used, 1 if the step was committed */
 int a2d_case_scalars(const a2d_plan* plan, double* out, void* stream);
+/* forces of every case at the current U to host arrays: coef [ncases][3] = Cl, Cd, Cm
+ * (euler.py:318-331), cp [sum of ni] or NULL; synchronises */
+int a2d_case_forces(a2d_plan* plan, double* coef, double* cp, void* stream);
+/* restarts the listed cases (host index list) with new freestreams winf [n][4]: U := the
+ * freestream state unless keep_state (then the current U is the start, as U0 of
+ * implicit.py:194-253), Newton state reset as a2d_reset, the cases live again; the
+ * other cases are untouched.  With keep_state a case that has stepped keeps its residual
+ * reference r0 (the previous point's), so params.tol keeps its absolute level and the
+ * SER CFL ramp starts at once; a2d_reset after U0 instead takes r0 from the first
+ * residual, as the reference does.  The slot recycling of a served batch. */
+int a2d_case_restart(a2d_plan* plan, int n, const int* cases, const double* winf, int keep_state, void* stream);
+/* stops the listed cases (host index list) from stepping until they are restarted */
+int a2d_case_retire(a2d_plan* plan, int n, const int* cases, void* stream);
+
+/* ---- continuous-batching service: served polar sweeps on one grid ----
+ * A fixed number of slots share one grid.  A request is a sequence of freestreams
+ * (e.g. the points of an alpha sweep) solved one after another in one slot, each point
+ * from the previous point's state when `continuation` is set (alpha continuation), else
+ * from the freestream; a point ends when it converges (drop below params.tol), freezes,
+ * or reaches params.max_iter steps.  A slot freed by a finished request is refilled from
+ * the queue before the next Newton step.  No counterpart exists in the reference (its
+ * callers loop over ImplicitEuler.solve); the C ABI's own serving entry points. */
+typedef struct a2d_service a2d_service;
+/* ni, nc: cells of the grid (as a2d_plan_create); metrics: its blob (a2d_metrics_build) */
+int a2d_service_create(int ni, int nc, const void* metrics, int slots, const a2d_params* params,
+                       a2d_service** service);
+int a2d_service_workspace_bytes(const a2d_service* service, size_t* bytes);
+int a2d_service_bind(a2d_service* service, void* workspace, size_t bytes, void* stream);
+/* winf: host [npoints][4]; *id receives the request id (> 0) */
+int a2d_service_submit(a2d_service* service, int npoints, const double* winf, int continuation, long long* id);
+/* admits queued requests, takes one Newton step of the busy slots and collects the
+ * points that ended; *busy receives the busy slots before the step; synchronises */
+int a2d_service_step(a2d_service* service, int* busy, void* stream);
+/* ids of requests finished since the last poll (at most max_ids) */
+int a2d_service_poll(a2d_service* service, long long* ids, int max_ids, int* n);
+/* a finished request's results to host arrays: coef [npoints][3], cp [npoints][ni] or NULL,
+ * converged [npoints], nsteps [npoints]; releases the request */
+int a2d_service_result(a2d_service* service, long long id, double* coef, double* cp, int* converged, int* nsteps);
+int a2d_service_pending(a2d_service* service, int* queued, int* running);
+int a2d_service_destroy(a2d_service* service);
 /* per-step histories to host arrays [steps][ncases] (residual norm, Cl); steps <= max_iter */
 int a2d_history(const a2d_plan* plan, int steps, double* rn, double* cl, void* stream);
 
