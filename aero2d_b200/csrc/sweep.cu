@@ -22,11 +22,15 @@
 // run per row: fbidx/fbidx3, a consumer's block row is one vector load) into a
 // ring of kStages stages per half with two mbarriers per stage: "full" (the
 // bulk-copy bytes) and "empty" (one arrival per consumer warp that is done with
-// the stage).  The consumers copy the vector entries of the forward steps into
-// the same stages by per-thread cp.async, kStages steps ahead, and compute: a
-// line's 4-vector passes between the four row warps of a half
-// through a two-slot exchange buffer with one named barrier per step, and the
-// halves meet twice around the twist row.  d_j goes to x (the last sweep, whose
+// the stage).  Each consumer thread loads its own vector entries of the forward
+// steps (component q of its line) through L2 into registers kAhead steps ahead
+// and stores them into a two-slot shared buffer the step before they are used,
+// so that the step's barrier publishes them to the other row warps; a line's
+// 4-vector passes between the four row warps of a half through a two-slot
+// exchange buffer, one named barrier per step, and the halves meet twice
+// around the twist row.  (Per-thread L1-allocating cp.async copies of the
+// vectors written by the preceding sweep were measured to return stale data
+// now and then, so these loads bypass L1.)  d_j goes to x (the last sweep, whose
 // x is FP64: to a scratch vector) and comes back, register-prefetched, in the
 // back substitution.  Every wait is bounded; a wait that runs out records an
 // error and the CTA drains its copies in flight (bounded again) before exit.
@@ -56,12 +60,14 @@ template <typename TI> struct SweepTypes;
 template <> struct SweepTypes<float> {
   using TF = __half;
   using TC = float;
-  static constexpr int kStages = 4;   // per half
+  static constexpr int kStages = 4;   // bulk-copy ring stages per half
+  static constexpr int kAhead = 2;    // steps between loading a vector entry and its use
 };
 template <> struct SweepTypes<double> {
   using TF = double;
   using TC = double;
   static constexpr int kStages = 2;
+  static constexpr int kAhead = 2;
 };
 
 template <typename TI>
@@ -78,7 +84,7 @@ struct SweepSmem {
       (3 * kLanes * 4 * sizeof(TC) > kLanes * 4 * sizeof(double)) ? 3 * kLanes * 4 * sizeof(TC)
                                                                    : kLanes * 4 * sizeof(double);
   alignas(128) unsigned char mat[2][kS][kMatBytes];
-  alignas(16) unsigned char vec[2][kS][kVecBytes];
+  alignas(16) unsigned char vec[2][2][kVecBytes];   // per half, by step parity
   alignas(16) TC xchg[2][2][kLanes][4];   // per half: the previous step's 4-vector of every line
   alignas(16) TC xk[kLanes][4];           // the twist row's solution
   uint64_t full[2][kS];
@@ -108,10 +114,6 @@ __device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
   const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
   v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
 }
-
-// asynchronous copy of one vector entry
-__device__ __forceinline__ void async_copy_entry(float* dst, const float* src) { async_copy4(dst, src); }
-__device__ __forceinline__ void async_copy_entry(double* dst, const double* src) { async_copy8(dst, src); }
 
 // barrier of the 128 consumer threads of one half (ids 1, 2) and of all 256
 // consumer threads (id 3); the producer warp takes part in none
@@ -249,23 +251,36 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   const TC* xpv = reinterpret_cast<const TC*>(a.xprev) + vq;
   const double* rv = a.r + vq;
 
-  // the vector entries of step t (forward steps and the twist row): each thread
-  // copies component q of its line into the stage; one cp.async group per step,
-  // empty ones included, keeps the group count regular
-  auto issue_vec = [&](int t) {
-    if (t < nf || (h == 0 && t == k)) {
-      const int s = t % S;
-      const size_t row = (size_t)row_of(h, t) * ni;
+  // the vector entries of step u (forward steps and the twist row): each thread
+  // loads component q of its line (r, or e0 and x' of both neighbour lines)
+  // into register slot sl and later stores it into the step's parity slot
+  constexpr int L = SweepTypes<TI>::kAhead;
+  double rr[L];
+  TC re[L], rm[L], rp[L];
+  auto has_vec = [&](int u) { return u < nf || (h == 0 && u == k); };
+  auto load_vec = [&](int u, int sl) {
+    if (has_vec(u)) {
+      const size_t row = (size_t)row_of(h, u) * ni;
       if constexpr (FIRST) {
-        async_copy8(reinterpret_cast<double*>(sm.vec[h][s]) + l * 4 + q, rv + row + i);
+        rr[sl] = __ldcg(rv + row + i);
       } else {
-        TC* v = reinterpret_cast<TC*>(sm.vec[h][s]) + l * 4 + q;
-        async_copy_entry(v, e0v + row + i);
-        async_copy_entry(v + kLanes * 4, xpv + row + im);
-        async_copy_entry(v + 2 * kLanes * 4, xpv + row + ip);
+        re[sl] = __ldcg(e0v + row + i);
+        rm[sl] = __ldcg(xpv + row + im);
+        rp[sl] = __ldcg(xpv + row + ip);
       }
     }
-    async_commit();
+  };
+  auto store_vec = [&](int u, int sl) {
+    if (has_vec(u)) {
+      if constexpr (FIRST) {
+        reinterpret_cast<double*>(sm.vec[h][u & 1])[l * 4 + q] = rr[sl];
+      } else {
+        TC* v = reinterpret_cast<TC*>(sm.vec[h][u & 1]) + l * 4 + q;
+        v[0] = re[sl];
+        v[kLanes * 4] = rm[sl];
+        v[2 * kLanes * 4] = rp[sl];
+      }
+    }
   };
 
   // waits for stage t of the half; a wait that runs out marks the step's
@@ -278,20 +293,21 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty[h][t % S]);
   };
-  // e_j of stage s from the forward blocks and vector entries
-  auto rhs = [&](int s, int j) -> TC {
+  // e_j of step t from the forward blocks of stage s and the step's vector entries
+  auto rhs = [&](int t, int s, int j) -> TC {
     const unsigned char* m = sm.mat[h][s];
+    const unsigned char* vsb = sm.vec[h][t & 1];
     TC e;
     if constexpr (FIRST) {
-      TC iv[4], rv[4];
+      TC iv[4], rvv[4];
       load4(reinterpret_cast<const TI*>(m) + eo, iv);
-      load4(reinterpret_cast<const double*>(sm.vec[h][s]) + l * 4, rv);
-      e = iv[0] * rv[0];
+      load4(reinterpret_cast<const double*>(vsb) + l * 4, rvv);
+      e = iv[0] * rvv[0];
 #pragma unroll
-      for (int c = 1; c < 4; ++c) e += iv[c] * rv[c];
+      for (int c = 1; c < 4; ++c) e += iv[c] * rvv[c];
       if (a.e0 != nullptr && owner) reinterpret_cast<TC*>(a.e0)[vq + (size_t)j * ni + i] = e;
     } else {
-      const TC* vs = reinterpret_cast<const TC*>(sm.vec[h][s]);
+      const TC* vs = reinterpret_cast<const TC*>(vsb);
       TC pv[4], qv[4], xm[4], xp[4];
       load4(reinterpret_cast<const TF*>(m) + eo, pv);
       load4(reinterpret_cast<const TF*>(m + kBytesF) + eo, qv);
@@ -309,35 +325,40 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     return e;
   };
 
-#pragma unroll 1
-  for (int t = 0; t < S; ++t) issue_vec(t);
-  async_wait<S - 1>();
-  half_sync(h);       // vector entries of step 0 visible to the half
+  // step 0's entries stored, steps 1 .. L in flight
+  load_vec(0, 0);
+  store_vec(0, 0);
+#pragma unroll
+  for (int u = 1; u <= L; ++u) load_vec(u, u % L);
+  half_sync(h);
 
   int tstop = -1;     // step at which a wait ran out
-  // ---- forward eliminations of both halves ----
+  // ---- forward eliminations of both halves (unrolled by L: register slots are static) ----
 #pragma unroll 1
-  for (int t = 0; t < nf; ++t) {
-    const int s = t % S;
-    const int j = row_of(h, t);
-    wait_full(t);
-    const TC e = rhs(s, j);
-    TC gv[4], dp[4];
-    load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
-    release(t);
-    load4(&sm.xchg[h][(t + 1) & 1][l][0], dp);
-    TC d = e;
+  for (int tb = 0; tb < nf && tstop < 0; tb += L) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
-    sm.xchg[h][t & 1][l][q] = d;
-    if (owner) dv[(size_t)j * ni + i] = d;
-    async_wait<S - 2>();   // this thread's entries of step t+1 landed; the barrier publishes them
-    half_sync(h);
-    if (sm.abort[h][t & 1]) {
-      tstop = t;
-      break;
+    for (int uu = 0; uu < L; ++uu) {
+      const int t = tb + uu;
+      if (t < nf && tstop < 0) {
+        const int s = t % S;
+        const int j = row_of(h, t);
+        wait_full(t);
+        const TC e = rhs(t, s, j);
+        TC gv[4], dp[4];
+        load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
+        release(t);
+        load4(&sm.xchg[h][(t + 1) & 1][l][0], dp);
+        TC d = e;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
+        sm.xchg[h][t & 1][l][q] = d;
+        if (owner) dv[(size_t)j * ni + i] = d;
+        store_vec(t + 1, (uu + 1) % L);      // step t+1's entries, published by the barrier
+        load_vec(t + 1 + L, (uu + 1) % L);   // and the slot refilled L steps ahead
+        half_sync(h);
+        if (sm.abort[h][t & 1]) tstop = t;
+      }
     }
-    issue_vec(t + S);
   }
   if (tstop >= 0 && l == 0 && q == 0) sm.failed[h] = 1;
   consumers_sync();   // (A) both forward eliminations done
@@ -346,7 +367,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     const int t = k;
     const int s = t % S;
     wait_full(t);
-    const TC e = rhs(s, k);
+    const TC e = rhs(t, s, k);
     TC gv[4], hv[4], dm[4], dpl[4];
     load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
     load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffH) + eo, hv);
@@ -411,7 +432,6 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
 #pragma unroll 1
     for (int u = tstop; u < tstop + S && u < nsteps; ++u) (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
   }
-  if (tstop >= 0) async_wait<0>();   // this thread's own vector copies land before it exits
 }
 
 template <typename TI, bool FIRST>

@@ -1,7 +1,7 @@
 // Asynchronous global -> shared copies for sm_100a: 1-D bulk copies (TMA
-// engine, completion counted in bytes on an mbarrier) and per-thread 8-byte
-// cp.async copies (completion by commit groups).  No cluster multicast is
-// used anywhere: every copy lands in the issuing CTA's own shared memory.
+// engine, completion counted in bytes on an mbarrier) and the mbarrier
+// operations around them.  No cluster multicast is used anywhere: every copy
+// lands in the issuing CTA's own shared memory.
 //
 // Every wait here is bounded by wall time (%globaltimer); a wait that runs
 // out returns false and the caller records the failure and leaves cleanly.
@@ -71,33 +71,9 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
       : "memory");
 }
 
-// 8-byte asynchronous copy, global -> shared, by the calling thread
-__device__ __forceinline__ void async_copy8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-
-// 4-byte asynchronous copy, global -> shared, by the calling thread
-__device__ __forceinline__ void async_copy4(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-
-__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-
-// one arrival on `bar`, triggered once every cp.async the calling thread issued
-// before it has completed (the arrival counts toward the expected count)
-__device__ __forceinline__ void async_arrive(uint64_t* bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // one plain arrival (no transaction bytes)
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// waits until at most N of the calling thread's committed groups are pending
-template <int N>
-__device__ __forceinline__ void async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 }  // namespace a2d

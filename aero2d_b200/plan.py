@@ -38,13 +38,24 @@ class DeviceGrid:
     """An O-grid resident on the device: node coordinates and the metrics blob
     (cell areas, face vectors, wall and far-field face midpoints, FP64 and FP32)."""
 
-    def __init__(self, grid: OGrid, device=None):
+    def __init__(self, grid: OGrid | None = None, device=None, *, nodes: tuple | None = None):
+        """From a host OGrid, or from node coordinates already on the device
+        (`nodes=(x, y)`, contiguous FP64 tensors (ni, nj), as the device grid
+        generator writes them)."""
         lib = _lib.load()
-        self.device = device_of(device)
-        ni, nj = grid.shape
+        if nodes is not None:
+            self.x, self.y = nodes
+            self.device = self.x.device
+            if self.x.dtype != torch.float64 or self.x.shape != self.y.shape or self.x.dim() != 2 \
+                    or not (self.x.is_contiguous() and self.y.is_contiguous()):
+                raise ValueError("nodes must be two contiguous float64 (ni, nj) device tensors")
+            ni, nj = self.x.shape
+        else:
+            self.device = device_of(device)
+            ni, nj = grid.shape
+            self.x = torch.as_tensor(np.ascontiguousarray(grid.x, np.float64), device=self.device)
+            self.y = torch.as_tensor(np.ascontiguousarray(grid.y, np.float64), device=self.device)
         self.ni, self.nj, self.nc = ni, nj, nj - 1
-        self.x = torch.as_tensor(np.ascontiguousarray(grid.x, np.float64), device=self.device)
-        self.y = torch.as_tensor(np.ascontiguousarray(grid.y, np.float64), device=self.device)
         n = C.c_size_t()
         _lib.check(lib.a2d_metrics_bytes(ni, nj, C.byref(n)))
         self.metrics = torch.empty(n.value, dtype=torch.uint8, device=self.device)

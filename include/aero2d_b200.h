@@ -74,6 +74,17 @@ int a2d_version(void);
 const char* a2d_last_error(void);
 void a2d_default_params(a2d_params* params);
 
+/* ---- O-grid generation on the device (aero2d/grid.py:34-81 ogrid, growth ratio) ----
+ * a2d_grid_spacing: host; spacing[k] = ds0 * r**k for k < nj - 1, r from 200 bisection steps
+ * (grid.py:34-41, :52-53).  a2d_grid_build: n grids at once, one CTA each (grid.py:50-81):
+ * ring device [n][ni][2] contour points (trailing-edge point once, 3 <= ni <= 1024), spacing
+ * device [n][nj-1], outputs x, y device [n][ni][nj] and min_area device [n] (the smallest cell
+ * area; <= 0 is the reference's inverted-grid RuntimeError, grid.py:78-80).  Layers 0..nj-2 are
+ * bitwise the reference's marching; the outer circle uses the device's atan2/cos/sin. */
+int a2d_grid_spacing(int nj, double ds0, double radius, double* spacing);
+int a2d_grid_build(int n, int ni, int nj, const double* ring, const double* spacing, int normal_smoothing,
+                   double* x, double* y, double* min_area, void* stream);
+
 /* ---- grid metrics (aero2d/euler.py:44-60 compute_metrics, :230-233 xf/yf) ---- */
 int a2d_metrics_bytes(int ni, int nj, size_t* bytes);
 /* x, y: device FP64 node coordinates [ni][nj]; metrics: device blob of a2d_metrics_bytes */

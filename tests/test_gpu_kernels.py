@@ -160,3 +160,44 @@ def test_smoothing_vs_fft(cuda):
     Ro = om.smooth(R)
     Rs = s.smooth(torch.as_tensor(R)).cpu().numpy()
     assert np.max(np.abs(Rs - Ro)) / np.max(np.abs(Ro)) < 1e-12
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_precond_and_step_repeatable(cuda, mixed):
+    """The line preconditioner and a whole Newton step are pure functions of
+    their inputs: on the 256 x 64 benchmark grid with 16 cases and 4 sweeps,
+    two inputs applied alternately give bitwise the same output every time, and
+    a Newton step repeated from the same state gives the same update.  (Large
+    enough that the sweep kernels fill the GPU; small grids hide scheduling
+    effects.)"""
+    from aero2d_b200.geometry import naca4
+    from aero2d_b200.grid import ogrid
+    g = ogrid(naca4("2412", 129), nj=65, ds0=2e-3, radius=20.0)
+    rng = np.random.default_rng(5)
+    B = 16
+    base = EulerSolver(g, dtype=np.float32 if mixed else np.float64, device=cuda)
+    w = base.freestream(rng.uniform(0.3, 0.75, B), rng.uniform(-4, 8, B))
+    pl = Plan([base.dgrid] * B, w, base.params(gmres_restart=30, jacobi_sweeps=4), cuda)
+    pl.init_freestream()
+    for _ in range(3):
+        pl.newton_step()
+    shape = (B, 4, g.shape[0], g.shape[1] - 1)
+    Va = torch.as_tensor(rng.standard_normal(shape), device=cuda)
+    Vb = torch.as_tensor(rng.standard_normal(shape), device=cuda)
+    pl.precond_setup()
+    outs = {0: [], 1: []}
+    for r in range(12):
+        pl.set_batch(_lib.VEC_V, Va if r % 2 == 0 else Vb)
+        pl.precond_apply()
+        outs[r % 2].append(pl.get_batch(_lib.VEC_JV))
+    for o in outs.values():
+        assert all(torch.equal(x, o[0]) for x in o[1:])
+    U = pl.get_batch(_lib.VEC_U).clone()
+    dus = []
+    for _ in range(4):
+        pl.set_batch(_lib.VEC_U, U)
+        pl.reset()
+        pl.newton_step()
+        dus.append(pl.get_batch(_lib.VEC_DU))
+    assert all(torch.equal(d, dus[0]) for d in dus[1:])
+    pl.close()

@@ -72,3 +72,29 @@ def test_run_euler_known_answer(cuda, known_answers):
     pc = run_euler("0012", [0.0, 2.0], 0.5, grid="coarse", n_iter=100, continuation=True, device=cuda)
     assert pc.ok.all()
     assert np.max(np.abs(pc.cl - p.cl)) < 4e-4
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_service_result_same_alone_and_in_the_mix(cuda, dtype):
+    """A request's results do not depend on what else is being served: alone in
+    a one-slot service and admitted late into a busy three-slot service, its
+    points come out bitwise the same (every reduction is per case and in a
+    fixed order; slots share no state)."""
+    g = grid("0012", 33, 25)
+    kw = dict(dtype=dtype, device=cuda, tol=1e-8, max_iter=120)
+    alone = EulerService(g, slots=1, **kw)
+    rid = alone.submit(0.55, [1.0, 3.0, 5.0])
+    alone.run()
+    ra = alone.result(rid)
+    alone.close()
+    mix = EulerService(g, slots=3, **kw)
+    others = [mix.submit(0.4, [0.0, 2.0]), mix.submit(0.7, [2.0]), mix.submit(0.3, [-3.0, 0.0, 3.0])]
+    for _ in range(7):
+        mix.step()
+    rid = mix.submit(0.55, [1.0, 3.0, 5.0])
+    done = mix.run()
+    assert rid in done and all(o in done for o in others)
+    rm = mix.result(rid)
+    mix.close()
+    for key in ("cl", "cd", "cm", "cp", "converged", "nsteps"):
+        assert np.array_equal(ra[key], rm[key]), key

@@ -88,3 +88,13 @@ def test_plan_rejects_bad_params():
     w = (C.c_double * 4)(1.0, 0.5, 0.0, 1 / 1.4)
     assert lib.a2d_plan_create(1, ni, nc, m, w, C.byref(p), C.byref(h)) == _lib.A2D_ERR_ARG
     assert b"gmres_restart" in lib.a2d_last_error()
+
+
+@pytest.mark.parametrize("nj,ds0,radius", [(25, 2e-3, 40.0), (49, 2e-3, 40.0), (65, 2e-3, 20.0), (97, 1e-3, 20.0)])
+def test_device_grid_spacing_matches_host(nj, ds0, radius):
+    """The C ABI's layer spacings (host C++) against the host generator's."""
+    from aero2d_b200.gridgen import layer_spacing
+    out = np.empty(nj - 1)
+    _lib.check(_lib.load().a2d_grid_spacing(nj, ds0, radius, out.ctypes.data_as(C.POINTER(C.c_double))))
+    ref = layer_spacing(nj, ds0, radius)
+    assert np.max(np.abs(out - ref) / ref) <= 2.3e-16
