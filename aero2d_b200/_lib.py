@@ -114,6 +114,10 @@ SIGNATURES = {
     "a2d_service_result": (_I, [_P, C.c_longlong, C.POINTER(_D), C.POINTER(_D), C.POINTER(_I), C.POINTER(_I)]),
     "a2d_service_pending": (_I, [_P, C.POINTER(_I), C.POINTER(_I)]),
     "a2d_service_destroy": (_I, [_P]),
+    "a2d_case_set_grid": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_P), _P]),
+    "a2d_service_create_ragged": (_I, [_I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_P), C.POINTER(_I),
+                                       C.POINTER(Params), C.POINTER(_P)]),
+    "a2d_service_submit_grid": (_I, [_P, _I, _I, _P, _I, C.POINTER(_D), _I, C.POINTER(C.c_longlong)]),
     "a2d_grid_spacing": (_I, [_I, _D, _D, C.POINTER(_D)]),
     "a2d_grid_build": (_I, [_I, _I, _I, _P, _P, _I, _P, _P, _P, _P]),
 }

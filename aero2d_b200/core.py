@@ -100,8 +100,9 @@ def run_euler(af, alphas, mach: float, grid: str = "грубая (быстро)"
         svc.run()
         r = svc.result(rid)
         cl, cd, cm, cp, ok, nsteps = r["cl"], r["cd"], r["cm"], r["cp"], r["converged"], r["nsteps"]
-        xw = np.asarray(svc.base.m_np.xw)
         svc.close()
+        from .euler import compute_metrics
+        xw = np.asarray(compute_metrics(g).xw)
     else:
         # lockstep like the reference's loop: every angle steps until all are done, so an angle
         # that converges early is iterated further exactly as the reference returns it

@@ -795,6 +795,25 @@ int a2d_case_forces(a2d_plan* P, double* coef, double* cp, void* stream) {
   return A2D_OK;
 }
 
+int a2d_case_set_grid(a2d_plan* P, int n, const int* cases, const void* const* metrics, void* stream) {
+  A2D_BOUND(P);
+  if (n < 0 || n > P->ncases || (n > 0 && (cases == nullptr || metrics == nullptr)))
+    return fail(A2D_ERR_ARG, "case_set_grid: bad arguments");
+  if (n == 0) return A2D_OK;
+  for (int q = 0; q < n; ++q) {
+    const int k = cases[q];
+    if (k < 0 || k >= P->ncases) return fail(A2D_ERR_ARG, "case_set_grid: case index out of range");
+    if (metrics[q] == nullptr) return fail(A2D_ERR_ARG, "case_set_grid: null metrics");
+  }
+  for (int q = 0; q < n; ++q) {
+    CaseDev& c = P->cases[cases[q]];
+    c.g = grid_view(metrics[q], c.g.ni, c.g.nc);
+  }
+  A2D_CK(cudaMemcpyAsync(P->ws + P->o_cases, P->cases.data(), sizeof(CaseDev) * P->ncases, cudaMemcpyHostToDevice,
+                         static_cast<cudaStream_t>(stream)));
+  return A2D_OK;
+}
+
 int a2d_case_retire(a2d_plan* P, int n, const int* cases, void* stream) {
   A2D_BOUND(P);
   if (n < 0 || n > P->ncases || (n > 0 && cases == nullptr)) return fail(A2D_ERR_ARG, "case_retire: bad arguments");

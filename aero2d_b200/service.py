@@ -1,57 +1,117 @@
-"""Continuous-batching Euler service: served polar sweeps on one grid.
+"""Continuous-batching Euler service: served polar sweeps.
 
-A fixed number of slots of one batched Newton-Krylov plan share an O-grid.  A
-request is a polar sweep -- a Mach number and a list of angles of attack --
-solved point after point in one slot, each point started from the previous
-point's state (alpha continuation) unless `continuation=False`; a slot freed
-by a finished request is refilled from the queue before the next Newton step,
-so the batch stays full instead of draining to its slowest case (the serving
-pattern of the reference's polar callers, which loop over
-ImplicitEuler.solve: aero2d/core.py:220-260).  The work runs in the library's
-C ABI (a2d_service_*, include/aero2d_b200.h); this class owns the device
-workspace and converts (M, alpha) to freestreams with EulerSolver.freestream.
+The slots of one batched Newton-Krylov plan are grouped in classes by grid
+size.  A request is a polar sweep -- a Mach number and a list of angles of
+attack -- on one grid, solved point after point in one slot of that grid's
+size, each point started from the previous point's state (alpha continuation)
+unless `continuation=False`.  Before every Newton step, queued requests are
+admitted in arrival order into free slots of their class, so the batch stays
+full instead of draining to its slowest case (the serving pattern of the
+reference's polar callers, which loop over ImplicitEuler.solve:
+aero2d/core.py:220-260).  A request can bring its own grid (a DeviceGrid of a
+class's size, e.g. from gridgen.ogrid_batch for a new airfoil); the service
+keeps it alive until the request's result is taken.  The work runs in the
+library's C ABI (a2d_service_*, include/aero2d_b200.h); this class owns the
+device workspace.
 
-    svc = EulerService(grid, slots=64)
-    rid = svc.submit(0.5, np.arange(-4, 17, 1.0))
+    svc = EulerService(grid, slots=64)                       # one grid size
+    svc = EulerService(classes=[(g128, 16), (g256, 16)])     # ragged slots
+    rid = svc.submit(0.5, np.arange(-4, 17, 1.0), grid=dg)   # dg: that request's grid
     done = svc.run()                 # or svc.step() in your own loop + svc.poll()
     res = svc.result(rid)            # dict: alpha, cl, cd, cm, cp, converged, nsteps
 """
 from __future__ import annotations
 
 import ctypes as C
-from typing import Optional
+from typing import Optional, Sequence
 
 import numpy as np
 import torch
 
 from . import _lib
-from .euler import EulerSolver
+from .euler import GAMMA, _precision_of
 from .grid import OGrid
 from .plan import DeviceGrid, _ptr, device_of, stream_handle
 
 
-class EulerService:
-    def __init__(self, grid: OGrid, slots: int = 64, dtype=np.float32, device=None, tol: float = 1e-8,
-                 max_iter: int = 200, gmres_restart: int = 30, cfl0: float = 10.0, cfl_max: float = 300.0,
-                 gmres_tol: float = 0.01, jacobi_sweeps: int = 4, max_update: float = 0.2):
-        self.device = device_of(device)
-        self.base = EulerSolver(grid, dtype=dtype, device=self.device)
-        self.dgrid: DeviceGrid = self.base.dgrid
-        self.slots = int(slots)
-        p = self.base.params(gmres_restart=int(gmres_restart), gmres_tol=float(gmres_tol), cfl0=float(cfl0),
-                             cfl_max=float(cfl_max), max_update=float(max_update), tol=float(tol),
-                             jacobi_sweeps=int(jacobi_sweeps), max_iter=int(max_iter), retire=1)
-        self.lib = _lib.load()
+def freestream(mach, alpha_deg) -> np.ndarray:
+    """Freestream primitives (rho, u, v, p) per point (aero2d/euler.py:253-256)."""
+    mach = np.asarray(mach, np.float64)
+    a = np.deg2rad(np.asarray(alpha_deg, np.float64))
+    one = np.ones_like(mach)
+    return np.stack([one, mach * np.cos(a), mach * np.sin(a), one / GAMMA], axis=-1)
+
+
+def workspace_bytes_per_slot(ni: int, nc: int, gmres_restart: int = 30, dtype=np.float32) -> int:
+    """Device bytes one slot of an ni x nc grid takes in a service workspace
+    (host-side query: no device memory is touched)."""
+    lib = _lib.load()
+    p = _lib.default_params()
+    p.gmres_restart = int(gmres_restart)
+    p.precision = _precision_of(dtype)
+    sizes = []
+    for n in (1, 2):
         h = C.c_void_p()
-        _lib.check(self.lib.a2d_service_create(self.dgrid.ni, self.dgrid.nc, C.c_void_p(self.dgrid.ptr), self.slots,
-                                               C.byref(p), C.byref(h)))
+        _lib.check(lib.a2d_plan_create(n, (C.c_int * n)(*[ni] * n), (C.c_int * n)(*[nc] * n),
+                                       (C.c_void_p * n)(*[1] * n), (C.c_double * (4 * n))(*([1.0, 0.5, 0.0, 0.7] * n)),
+                                       C.byref(p), C.byref(h)))
+        b = C.c_size_t()
+        _lib.check(lib.a2d_plan_workspace_bytes(h, C.byref(b)))
+        lib.a2d_plan_destroy(h)
+        sizes.append(b.value)
+    return sizes[1] - sizes[0]
+
+
+def slots_for_budget(shapes: Sequence[tuple[int, int]], hbm_bytes: int, share: Optional[Sequence[float]] = None,
+                     gmres_restart: int = 30, dtype=np.float32) -> list[int]:
+    """Slots per grid size that fit `hbm_bytes` of workspace, the budget split
+    by `share` (default: equal bytes per size); at least one slot per size."""
+    share = np.full(len(shapes), 1.0 / len(shapes)) if share is None else np.asarray(share, float) / np.sum(share)
+    per = [workspace_bytes_per_slot(ni, nc, gmres_restart, dtype) for ni, nc in shapes]
+    return [max(1, int(hbm_bytes * s // b)) for s, b in zip(share, per)]
+
+
+class EulerService:
+    def __init__(self, grid: OGrid | DeviceGrid | None = None, slots: int = 64, dtype=np.float32, device=None,
+                 tol: float = 1e-8, max_iter: int = 200, gmres_restart: int = 30, cfl0: float = 10.0,
+                 cfl_max: float = 300.0, gmres_tol: float = 0.01, jacobi_sweeps: int = 4,
+                 max_update: float = 0.2, classes: Optional[Sequence[tuple]] = None):
+        """`grid` + `slots` for one grid size, or `classes` = [(grid, slots), ...]
+        with one grid per size (the class's default grid)."""
+        if classes is None:
+            if grid is None:
+                raise ValueError("give a grid (and slots) or classes")
+            classes = [(grid, slots)]
+        self.device = device_of(device)
+        self.classes = []
+        for g, n in classes:
+            dg = g if isinstance(g, DeviceGrid) else DeviceGrid(g, self.device)
+            self.classes.append((dg, int(n)))
+        shapes = [(dg.ni, dg.nc) for dg, _ in self.classes]
+        if len(set(shapes)) != len(shapes):
+            raise ValueError("each slot class needs its own grid size")
+        self._shape = {s: k for k, s in enumerate(shapes)}
+        p = _lib.default_params()
+        p.precision = _precision_of(dtype)
+        for k, v in dict(gmres_restart=int(gmres_restart), gmres_tol=float(gmres_tol), cfl0=float(cfl0),
+                         cfl_max=float(cfl_max), max_update=float(max_update), tol=float(tol),
+                         jacobi_sweeps=int(jacobi_sweeps), max_iter=int(max_iter), retire=1).items():
+            setattr(p, k, v)
+        self.lib = _lib.load()
+        m = len(self.classes)
+        h = C.c_void_p()
+        _lib.check(self.lib.a2d_service_create_ragged(
+            m, (C.c_int * m)(*[s[0] for s in shapes]), (C.c_int * m)(*[s[1] for s in shapes]),
+            (C.c_void_p * m)(*[dg.ptr for dg, _ in self.classes]), (C.c_int * m)(*[n for _, n in self.classes]),
+            C.byref(p), C.byref(h)))
         self.handle = h
         n = C.c_size_t()
         _lib.check(self.lib.a2d_service_workspace_bytes(h, C.byref(n)))
+        self.workspace_bytes = n.value
         self.workspace = torch.empty(n.value, dtype=torch.uint8, device=self.device)
         with torch.cuda.device(self.device):
             _lib.check(self.lib.a2d_service_bind(h, _ptr(self.workspace), n.value, self.stream))
-        self._meta: dict[int, tuple[float, np.ndarray]] = {}
+        self._meta: dict[int, tuple] = {}
 
     @property
     def stream(self) -> int:
@@ -68,17 +128,21 @@ class EulerService:
         except Exception:
             pass
 
-    def submit(self, mach: float, alphas, continuation: bool = True) -> int:
-        """Queues a sweep of `alphas` (degrees) at `mach`; returns the request id."""
+    def submit(self, mach: float, alphas, continuation: bool = True, grid: DeviceGrid | None = None) -> int:
+        """Queues a sweep of `alphas` (degrees) at `mach` on `grid` (a DeviceGrid
+        of a class's size; default: the first class's grid); returns the id."""
         alphas = np.atleast_1d(np.asarray(alphas, np.float64))
         if alphas.size == 0:
             raise ValueError("a request needs at least one angle of attack")
-        winf = np.ascontiguousarray(self.base.freestream(np.full(alphas.shape, float(mach)), alphas))
+        dg = grid if grid is not None else self.classes[0][0]
+        if (dg.ni, dg.nc) not in self._shape:
+            raise ValueError(f"no slot class for a {dg.ni} x {dg.nc} grid")
+        winf = np.ascontiguousarray(freestream(np.full(alphas.shape, float(mach)), alphas))
         rid = C.c_longlong()
-        _lib.check(self.lib.a2d_service_submit(self.handle, alphas.size,
-                                               winf.ctypes.data_as(C.POINTER(C.c_double)), int(bool(continuation)),
-                                               C.byref(rid)))
-        self._meta[rid.value] = (float(mach), alphas)
+        _lib.check(self.lib.a2d_service_submit_grid(self.handle, dg.ni, dg.nc, C.c_void_p(dg.ptr), alphas.size,
+                                                    winf.ctypes.data_as(C.POINTER(C.c_double)),
+                                                    int(bool(continuation)), C.byref(rid)))
+        self._meta[rid.value] = (float(mach), alphas, dg)
         return rid.value
 
     def step(self) -> int:
@@ -103,11 +167,11 @@ class EulerService:
         return q.value, r.value
 
     def result(self, rid: int) -> dict:
-        """A finished request's per-point results; releases the request."""
-        mach, alphas = self._meta.pop(rid)
+        """A finished request's per-point results; releases the request (and its grid)."""
+        mach, alphas, dg = self._meta[rid]
         n = alphas.size
         coef = np.empty((n, 3))
-        cp = np.empty((n, self.dgrid.ni))
+        cp = np.empty((n, dg.ni))
         conv = np.empty(n, np.int32)
         steps = np.empty(n, np.int32)
         _lib.check(self.lib.a2d_service_result(self.handle, C.c_longlong(rid),
@@ -115,6 +179,7 @@ class EulerService:
                                                cp.ctypes.data_as(C.POINTER(C.c_double)),
                                                conv.ctypes.data_as(C.POINTER(C.c_int)),
                                                steps.ctypes.data_as(C.POINTER(C.c_int))))
+        del self._meta[rid]
         return {"mach": mach, "alpha": alphas, "cl": coef[:, 0], "cd": coef[:, 1], "cm": coef[:, 2], "cp": cp,
                 "converged": conv.astype(bool), "nsteps": steps}
 

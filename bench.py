@@ -388,6 +388,10 @@ def gpu_arm(args, rank: int, world: int, dist):
     out["gpu_launches"] = int(launches)
     out["clocks"] = clk
 
+    # ---- served polar requests (continuous batching, ragged grids) ----------
+    if world == 1 and args.served_requests > 0:
+        out["served"] = served_arm(args, dev)
+
     # ---- CPU baseline ---------------------------------------------------------
     if world == 1 and not args.no_cpu_baseline:
         procs = max(1, min(os.cpu_count() or 1, args.cpu_procs))
@@ -399,6 +403,121 @@ def gpu_arm(args, rank: int, world: int, dist):
                                          f"{NEWTON_STEPS_PER_CASE} Newton steps per converged case",
                                "wall_s": round(cpu_wall, 1)}
     return out
+
+
+# served polar requests: the grid sizes of the ragged set (n_side, nj, ds0), radius 20
+SERVED_SIZES = [(65, 33, 2e-3), (97, 49, 2e-3), (129, 65, 2e-3), (193, 97, 1e-3)]
+SERVED_ALPHAS = np.arange(-4.0, 17.0, 1.0)
+
+
+def served_arm(args, dev):
+    """Served polar requests on one GPU: a seeded Poisson stream of requests,
+    each a 21-point alpha sweep (-4 .. 16 deg) at one random NACA 4-digit
+    airfoil (m ~ U[0, 0.06], p ~ U[0.2, 0.6], t ~ U[0.08, 0.16]; airfoils whose
+    grid folds are redrawn) on one grid size of the ragged set (128x32 ..
+    384x96, radius 20), M ~ U[0.2, 0.75], alpha continuation inside the
+    request, mixed precision, residual drop 1e-8 per point (at most
+    `served_max_iter` Newton steps).  Each request's grid is generated on the
+    device when it arrives; slots per grid size come from an HBM budget split
+    equally between the sizes.  Latency = arrival to the last point's result
+    (host wall clock: requests arrive in real time)."""
+    import torch
+    from aero2d_b200.geometry import naca4, naca4_params
+    from aero2d_b200.grid import GridError
+    from aero2d_b200.gridgen import ogrid_batch
+    from aero2d_b200.service import EulerService, slots_for_budget
+    rng = np.random.default_rng(SEED + 7)
+    n = args.served_requests
+    arrivals = np.cumsum(rng.exponential(1.0 / args.served_rate, n))
+    reqs, rejected = [], 0
+    while len(reqs) < n:
+        m, pp, t = rng.uniform(0, 0.06), rng.uniform(0.2, 0.6), rng.uniform(0.08, 0.16)
+        size = int(rng.integers(len(SERVED_SIZES)))
+        mach = rng.uniform(0.2, 0.75)
+        reqs.append((naca4_params(m, pp, t, SERVED_SIZES[size][0]), size, mach))
+    shapes = [(2 * ns - 2, nj - 1) for ns, nj, _ in SERVED_SIZES]
+    slots = slots_for_budget(shapes, args.served_hbm_gb * 1e9)
+    defaults = [ogrid_batch([naca4("0012", ns)], nj=nj, ds0=ds0, radius=20.0, device=dev)[0]
+                for ns, nj, ds0 in SERVED_SIZES]
+    svc = EulerService(classes=list(zip(defaults, slots)), dtype=np.float32, device=dev, tol=1e-8,
+                       max_iter=args.served_max_iter, gmres_restart=RESTART)
+    # warm the service (graph capture, first launches) with one short request
+    w = svc.submit(0.5, [2.0], grid=defaults[0])
+    svc.run()
+    svc.result(w)
+    rid_of, arr_of, grid_of, done_at = {}, {}, {}, {}
+    steps = 0
+    nxt = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while len(done_at) < n:
+        now = time.perf_counter() - t0
+        if now > args.served_wall_cap:
+            break
+        while nxt < n and arrivals[nxt] <= now:
+            af, size, mach = reqs[nxt]
+            ns, nj, ds0 = SERVED_SIZES[size]
+            while True:
+                try:
+                    (g,) = ogrid_batch([af], nj=nj, ds0=ds0, radius=20.0, device=dev)
+                    break
+                except GridError:
+                    rejected += 1
+                    af = naca4_params(rng.uniform(0, 0.06), rng.uniform(0.2, 0.6), rng.uniform(0.08, 0.16), ns)
+            rid = svc.submit(mach, SERVED_ALPHAS, continuation=True, grid=g)
+            rid_of[nxt], arr_of[rid], grid_of[rid] = rid, arrivals[nxt], (g, mach)
+            nxt += 1
+        busy = svc.step()
+        steps += busy > 0
+        for rid in svc.poll():
+            done_at[rid] = time.perf_counter() - t0
+        if busy == 0 and svc.pending()[0] == 0 and nxt < n:
+            time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
+    wall = time.perf_counter() - t0
+    res = {rid: svc.result(rid) for rid in done_at}
+    lat = np.array([done_at[r] - arr_of[r] for r in done_at])
+    conv = sum(int(r["converged"].sum()) for r in res.values())
+    pts = sum(r["converged"].size for r in res.values())
+    span = max(done_at.values()) - float(arrivals[0]) if done_at else float("nan")
+    svc.close()
+    # accuracy: the first two finished requests again in FP64, same grids and sweeps
+    acc_ids = sorted(done_at, key=done_at.get)[:2]
+    by_shape: dict = {}
+    for r in acc_ids:
+        by_shape.setdefault((grid_of[r][0].ni, grid_of[r][0].nc), []).append(r)
+    ref = EulerService(classes=[(grid_of[rs[0]][0], len(rs)) for rs in by_shape.values()], dtype=np.float64,
+                       device=dev, tol=1e-8, max_iter=args.served_max_iter, gmres_restart=RESTART)
+    rid64 = {r: ref.submit(grid_of[r][1], SERVED_ALPHAS, continuation=True, grid=grid_of[r][0]) for r in acc_ids}
+    ref.run()
+    dcl, dcd, ncmp = [], [], 0
+    for r, r64 in rid64.items():
+        a, b = res[r], ref.result(r64)
+        # points that reached the 1e-8 drop in both (the reference's converged flag asks only 1e-3)
+        both = a["converged"] & b["converged"] & (a["nsteps"] < args.served_max_iter) & \
+            (b["nsteps"] < args.served_max_iter)
+        ncmp += int(both.sum())
+        if both.any():
+            dcl.append(np.abs(a["cl"] - b["cl"])[both].max())
+            dcd.append(np.abs(a["cd"] - b["cd"])[both].max())
+    ref.close()
+    return {
+        "workload": f"{n} requests, Poisson arrivals at {args.served_rate:g}/s (seeded), 21-point alpha sweep "
+                    "-4..16 deg each with continuation, random NACA 4-digit airfoil and grid size "
+                    "(128x32, 192x48, 256x64, 384x96), M~U[0.2,0.75], mixed precision, drop 1e-8, "
+                    f"at most {args.served_max_iter} Newton steps per point, grids generated on the device",
+        "slots": dict(zip([f"{a}x{b}" for a, b in shapes], slots)),
+        "hbm_budget_gb": args.served_hbm_gb,
+        "requests_done": len(done_at), "grid_rejections": rejected,
+        "latency_s": {"p50": round(float(np.percentile(lat, 50)), 3), "p95": round(float(np.percentile(lat, 95)), 3),
+                      "p99": round(float(np.percentile(lat, 99)), 3)} if len(lat) else None,
+        "points": pts, "converged_points": conv,
+        "converged_points_per_s": round(conv / span, 3) if done_at else None,
+        "newton_steps": steps, "wall_s": round(wall, 2),
+        "accuracy_vs_fp64": {"max_abs_dCl": float(max(dcl)) if dcl else None,
+                             "max_abs_dCd": float(max(dcd)) if dcd else None, "points_compared": ncmp,
+                             "sample": "the first two finished requests re-served in FP64; points that reached "
+                                       "the 1e-8 drop in both"},
+    }
 
 
 def reference_arm(args):
@@ -460,6 +579,11 @@ def main():
     ap.add_argument("--single-sample", type=int, default=4)
     ap.add_argument("--cpu-procs", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=24, help="0 skips the served-requests measurement")
+    ap.add_argument("--served-rate", type=float, default=8.0, help="request arrivals per second")
+    ap.add_argument("--served-hbm-gb", type=float, default=2.0, help="workspace budget of the service")
+    ap.add_argument("--served-max-iter", type=int, default=100, help="Newton steps per point at most")
+    ap.add_argument("--served-wall-cap", type=float, default=150.0, help="seconds before the stream is cut")
     ap.add_argument("--profile", type=int, default=0, metavar="STEPS",
                     help="profiling driver: build the mixed plan, run STEPS Newton steps, print nothing")
     ap.add_argument("--fp64", action="store_true", help="with --profile: the all-FP64 plan")

@@ -151,23 +151,37 @@ int a2d_case_forces(a2d_plan* plan, double* coef, double* cp, void* stream);
 int a2d_case_restart(a2d_plan* plan, int n, const int* cases, const double* winf, int keep_state, void* stream);
 /* stops the listed cases (host index list) from stepping until they are restarted */
 int a2d_case_retire(a2d_plan* plan, int n, const int* cases, void* stream);
+/* points the listed cases at other grids of their size: metrics[q] is a device blob of
+ * a2d_metrics_build with case cases[q]'s ni, nc (kept alive by the caller while in use);
+ * a new airfoil for a served slot, followed by a2d_case_restart (cold) */
+int a2d_case_set_grid(a2d_plan* plan, int n, const int* cases, const void* const* metrics, void* stream);
 
-/* ---- continuous-batching service: served polar sweeps on one grid ----
- * A fixed number of slots share one grid.  A request is a sequence of freestreams
- * (e.g. the points of an alpha sweep) solved one after another in one slot, each point
- * from the previous point's state when `continuation` is set (alpha continuation), else
- * from the freestream; a point ends when it converges (drop below params.tol), freezes,
- * or reaches params.max_iter steps.  A slot freed by a finished request is refilled from
- * the queue before the next Newton step.  No counterpart exists in the reference (its
- * callers loop over ImplicitEuler.solve); the C ABI's own serving entry points. */
+/* ---- continuous-batching service: served polar sweeps ----
+ * A fixed set of slots, in classes by grid size (ni, nc).  A request is a sequence of
+ * freestreams (e.g. the points of an alpha sweep) on one grid of a class's size, solved one
+ * after another in one slot, each point from the previous point's state when `continuation`
+ * is set (alpha continuation), else from the freestream; a point ends when it converges (drop
+ * below params.tol), freezes, or reaches params.max_iter steps.  Before every Newton step,
+ * queued requests are admitted in arrival order into free slots of their class.  No
+ * counterpart exists in the reference (its callers loop over ImplicitEuler.solve); the C
+ * ABI's own serving entry points. */
 typedef struct a2d_service a2d_service;
-/* ni, nc: cells of the grid (as a2d_plan_create); metrics: its blob (a2d_metrics_build) */
+/* one class: ni, nc cells of the grid (as a2d_plan_create); metrics: its blob (a2d_metrics_build) */
 int a2d_service_create(int ni, int nc, const void* metrics, int slots, const a2d_params* params,
                        a2d_service** service);
+/* nclasses classes of distinct sizes: slots[c] slots of ni[c] x nc[c] cells each, metrics[c]
+ * the class's default grid (used by a2d_service_submit and by requests without a grid) */
+int a2d_service_create_ragged(int nclasses, const int* ni, const int* nc, const void* const* metrics,
+                              const int* slots, const a2d_params* params, a2d_service** service);
 int a2d_service_workspace_bytes(const a2d_service* service, size_t* bytes);
 int a2d_service_bind(a2d_service* service, void* workspace, size_t bytes, void* stream);
-/* winf: host [npoints][4]; *id receives the request id (> 0) */
+/* a request on the first class's default grid; winf: host [npoints][4]; *id receives the
+ * request id (> 0) */
 int a2d_service_submit(a2d_service* service, int npoints, const double* winf, int continuation, long long* id);
+/* a request on its own grid of ni x nc cells (a class's size): metrics is its device blob,
+ * kept alive by the caller until the request's result is taken (NULL: the class's default) */
+int a2d_service_submit_grid(a2d_service* service, int ni, int nc, const void* metrics, int npoints,
+                            const double* winf, int continuation, long long* id);
 /* admits queued requests, takes one Newton step of the busy slots and collects the
  * points that ended; *busy receives the busy slots before the step; synchronises */
 int a2d_service_step(a2d_service* service, int* busy, void* stream);

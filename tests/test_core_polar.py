@@ -41,3 +41,30 @@ def test_low_mach_rejected_before_any_device_work():
 def test_polar_record_fields():
     p = Polar("x", "euler", 0.5, np.zeros(2), np.zeros(2), np.zeros(2), np.zeros(2), np.ones(2, bool))
     assert p.method == "euler" and p.xref == (0.25, 0.0) and np.isnan(p.re)
+
+
+def test_service_slot_budget_on_host():
+    """Slot sizing and the ragged service's argument checks need no GPU."""
+    import ctypes as C
+    from aero2d_b200 import _lib
+    from aero2d_b200.service import slots_for_budget, workspace_bytes_per_slot
+    per = [workspace_bytes_per_slot(ni, nc) for ni, nc in [(128, 32), (192, 48), (256, 64), (384, 96)]]
+    assert all(b > 0 for b in per) and per == sorted(per)
+    n = slots_for_budget([(128, 32), (384, 96)], 10 * per[3], share=[1, 1])
+    assert n == [int(5 * per[3] // per[0]), 5]
+    lib = _lib.load()
+    h = C.c_void_p()
+    two = (C.c_int * 2)
+    st = lib.a2d_service_create_ragged(2, two(128, 128), two(32, 32), (C.c_void_p * 2)(1, 1), two(1, 1), None,
+                                       C.byref(h))
+    assert st == _lib.A2D_ERR_ARG          # two classes of one size
+    _lib.check(lib.a2d_service_create_ragged(2, two(128, 192), two(32, 48), (C.c_void_p * 2)(1, 1), two(2, 1), None,
+                                             C.byref(h)))
+    rid = C.c_longlong()
+    w = (C.c_double * 4)(1.0, 0.5, 0.0, 1 / 1.4)
+    assert lib.a2d_service_submit_grid(h, 256, 64, None, 1, w, 1, C.byref(rid)) == _lib.A2D_ERR_ARG
+    _lib.check(lib.a2d_service_submit_grid(h, 192, 48, None, 1, w, 1, C.byref(rid)))
+    q, r = C.c_int(), C.c_int()
+    _lib.check(lib.a2d_service_pending(h, C.byref(q), C.byref(r)))
+    assert (q.value, r.value) == (1, 0)
+    _lib.check(lib.a2d_service_destroy(h))

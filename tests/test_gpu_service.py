@@ -98,3 +98,35 @@ def test_service_result_same_alone_and_in_the_mix(cuda, dtype):
     mix.close()
     for key in ("cl", "cd", "cm", "cp", "converged", "nsteps"):
         assert np.array_equal(ra[key], rm[key]), key
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_ragged_service_alone_and_in_the_mix(cuda, dtype):
+    """Requests on different airfoils and two grid sizes, each grid built on
+    the device: every request's points are bitwise the same served alone (a
+    one-slot service of its size) and served in the ragged mix, where requests
+    wait for a slot of their size and are admitted as slots free up."""
+    from aero2d_b200.geometry import naca4
+    from aero2d_b200.gridgen import ogrid_batch
+    small = ogrid_batch([naca4(c, 33) for c in ("0012", "2412", "4415")], nj=25, ds0=2e-3, radius=20.0, device=cuda)
+    large = ogrid_batch([naca4(c, 49) for c in ("0012", "2412")], nj=33, ds0=2e-3, radius=20.0, device=cuda)
+    reqs = [(small[0], 0.5, [0.0, 2.0], True), (large[0], 0.6, [1.0, 3.0], True), (small[1], 0.4, [4.0], False),
+            (small[2], 0.55, [-2.0, 0.0, 2.0], True), (large[1], 0.3, [2.0], True)]
+    kw = dict(dtype=dtype, device=cuda, tol=1e-8, max_iter=120)
+    alone = []
+    for g, m, a, c in reqs:
+        s = EulerService(g, slots=1, **kw)
+        rid = s.submit(m, a, continuation=c, grid=g)
+        s.run()
+        alone.append(s.result(rid))
+        s.close()
+    mix = EulerService(classes=[(small[0], 2), (large[0], 1)], **kw)
+    ids = [mix.submit(m, a, continuation=c, grid=g) for g, m, a, c in reqs]
+    assert mix.pending()[0] == len(reqs)
+    done = mix.run()
+    assert sorted(done) == sorted(ids)
+    for rid, ra in zip(ids, alone):
+        rm = mix.result(rid)
+        for key in ("cl", "cd", "cm", "cp", "converged", "nsteps"):
+            assert np.array_equal(ra[key], rm[key]), key
+    mix.close()
