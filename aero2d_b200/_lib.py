@@ -114,6 +114,7 @@ SIGNATURES = {
     "a2d_service_result": (_I, [_P, C.c_longlong, C.POINTER(_D), C.POINTER(_D), C.POINTER(_I), C.POINTER(_I)]),
     "a2d_service_pending": (_I, [_P, C.POINTER(_I), C.POINTER(_I)]),
     "a2d_service_destroy": (_I, [_P]),
+    "a2d_plan_set_coarse": (_I, [_P, _P]),
     "a2d_case_set_grid": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_P), _P]),
     "a2d_service_create_ragged": (_I, [_I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_P), C.POINTER(_I),
                                        C.POINTER(Params), C.POINTER(_P)]),

@@ -188,6 +188,116 @@ __global__ void k_rk_finish(Batch b, const double* tpart, const double* coef, do
   circ[cs] = 0.5 * coef[3 * cs] * mach;
 }
 
+// ---------------------------------------------------------------------------
+// FAS multigrid transfers (aero2d/euler.py:349-381) between a fine batch and
+// the coarse batch of the same cases on grids of every other node (ni/2 x nc/2
+// cells).  Every sum and product is rounded separately, in the reference's
+// order, as the NumPy/JAX expressions evaluate them.
+// ---------------------------------------------------------------------------
+// R += P over the cells of every case (the forcing term of a coarse level)
+__global__ void __launch_bounds__(256) k_add_forcing(Batch b, double* __restrict__ R, const double* __restrict__ P) {
+  const Tile t = b.tiles[blockIdx.x];
+  const CaseDev cs = b.cases[t.cs];
+  const size_t base = 4 * cs.cell_off;
+  for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
+    const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const size_t q = base + vidx(cs.g, k, j, i);
+      R[q] = __dadd_rn(R[q], P[q]);
+    }
+  }
+}
+
+// sum4(a) = a(2i, 2j) + a(2i+1, 2j) + a(2i, 2j+1) + a(2i+1, 2j+1), left to right
+__device__ __forceinline__ double sum4(double a00, double a10, double a01, double a11) {
+  return __dadd_rn(__dadd_rn(__dadd_rn(a00, a10), a01), a11);
+}
+
+// one thread per coarse cell (tiles of the coarse batch): Uc = Uc0 = sum4(U vol) / sum4(vol);
+// with R != nullptr also Pc = sum4(R (+ P)) - Rc, where Rc is read from Pc (the coarse
+// residual at Uc0) and P (nullable) is the fine level's own forcing
+__global__ void __launch_bounds__(256) k_fas_restrict(Batch fb, Batch cb, const double* __restrict__ Uf,
+                                                     double* __restrict__ Uc, double* __restrict__ Uc0) {
+  const Tile t = cb.tiles[blockIdx.x];
+  const CaseDev cc = cb.cases[t.cs];
+  const CaseDev cf = fb.cases[t.cs];
+  const GridDev& gf = cf.g;
+  const size_t bf = 4 * cf.cell_off, bc = 4 * cc.cell_off;
+  for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
+    const int jc = t.j0 + c / t.ti, ic = t.i0 + c % t.ti;
+    const int i0 = 2 * ic, j0 = 2 * jc;
+    const double v00 = gf.vol[(size_t)j0 * gf.ni + i0], v10 = gf.vol[(size_t)j0 * gf.ni + i0 + 1];
+    const double v01 = gf.vol[(size_t)(j0 + 1) * gf.ni + i0], v11 = gf.vol[(size_t)(j0 + 1) * gf.ni + i0 + 1];
+    const double vs = sum4(v00, v10, v01, v11);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double* u = Uf + bf;
+      const double a = sum4(__dmul_rn(u[vidx(gf, k, j0, i0)], v00), __dmul_rn(u[vidx(gf, k, j0, i0 + 1)], v10),
+                            __dmul_rn(u[vidx(gf, k, j0 + 1, i0)], v01),
+                            __dmul_rn(u[vidx(gf, k, j0 + 1, i0 + 1)], v11));
+      const size_t q = bc + vidx(cc.g, k, jc, ic);
+      const double r = __ddiv_rn(a, vs);
+      Uc[q] = r;
+      Uc0[q] = r;
+    }
+  }
+}
+
+// Pc := sum4(Rf) - Pc (Pc holds the coarse residual at Uc0 on entry); Rf already includes
+// the fine level's forcing
+__global__ void __launch_bounds__(256) k_fas_forcing(Batch fb, Batch cb, const double* __restrict__ Rf,
+                                                    double* __restrict__ Pc) {
+  const Tile t = cb.tiles[blockIdx.x];
+  const CaseDev cc = cb.cases[t.cs];
+  const CaseDev cf = fb.cases[t.cs];
+  const GridDev& gf = cf.g;
+  const double* r = Rf + 4 * cf.cell_off;
+  const size_t bc = 4 * cc.cell_off;
+  for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
+    const int jc = t.j0 + c / t.ti, ic = t.i0 + c % t.ti;
+    const int i0 = 2 * ic, j0 = 2 * jc;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double a = sum4(r[vidx(gf, k, j0, i0)], r[vidx(gf, k, j0, i0 + 1)], r[vidx(gf, k, j0 + 1, i0)],
+                            r[vidx(gf, k, j0 + 1, i0 + 1)]);
+      const size_t q = bc + vidx(cc.g, k, jc, ic);
+      Pc[q] = __dsub_rn(a, Pc[q]);
+    }
+  }
+}
+
+// Uf += prolong(Uc - Uc0): in i 3/4 d(ic) + 1/4 d(ic -+ 1) (periodic), then in j
+// 3/4 a(jc) + 1/4 a(jc -+ 1) held at the ends (aero2d/euler.py:354-366); one thread
+// per fine cell
+__global__ void __launch_bounds__(256) k_fas_prolong(Batch fb, Batch cb, double* __restrict__ Uf,
+                                                    const double* __restrict__ Uc,
+                                                    const double* __restrict__ Uc0) {
+  const Tile t = fb.tiles[blockIdx.x];
+  const CaseDev cf = fb.cases[t.cs];
+  const CaseDev cc = cb.cases[t.cs];
+  const GridDev& gc = cc.g;
+  const size_t bf = 4 * cf.cell_off, bc = 4 * cc.cell_off;
+  for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
+    const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
+    const int ic = i >> 1, jc = j >> 1;
+    const int icn = (i & 1) ? (ic + 1 == gc.ni ? 0 : ic + 1) : (ic == 0 ? gc.ni - 1 : ic - 1);
+    const int jcn = (j & 1) ? (jc + 1 == gc.nc ? jc : jc + 1) : (jc == 0 ? 0 : jc - 1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      auto d = [&](int jj, int ii) {
+        const size_t q = bc + vidx(gc, k, jj, ii);
+        return __dsub_rn(Uc[q], Uc0[q]);
+      };
+      const double a0 = __dadd_rn(__dmul_rn(0.75, d(jc, ic)), __dmul_rn(0.25, d(jc, icn)));
+      const double a1 = __dadd_rn(__dmul_rn(0.75, d(jcn, ic)), __dmul_rn(0.25, d(jcn, icn)));
+      const double v = __dadd_rn(__dmul_rn(0.75, a0), __dmul_rn(0.25, a1));
+      const size_t q = bf + vidx(cf.g, k, j, i);
+      Uf[q] = __dadd_rn(Uf[q], v);
+    }
+  }
+}
+
 void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, cudaStream_t s) {
   if (b.ntiles) k_local_dt<<<b.ntiles, 256, 0, s>>>(b, U, dt, cfl);
 }
@@ -210,6 +320,21 @@ void launch_rk_res(const Batch& b, const double* U0, const double* U, const doub
 void launch_rk_finish(const Batch& b, const double* tpart, const double* coef, double* res, double* circ,
                       cudaStream_t s) {
   k_rk_finish<<<(b.ncases + 63) / 64, 64, 0, s>>>(b, tpart, coef, res, circ);
+}
+
+void launch_add_forcing(const Batch& b, double* R, const double* P, cudaStream_t s) {
+  if (b.ntiles) k_add_forcing<<<b.ntiles, 256, 0, s>>>(b, R, P);
+}
+void launch_fas_restrict(const Batch& fine, const Batch& coarse, const double* Uf, double* Uc, double* Uc0,
+                         cudaStream_t s) {
+  if (coarse.ntiles) k_fas_restrict<<<coarse.ntiles, 256, 0, s>>>(fine, coarse, Uf, Uc, Uc0);
+}
+void launch_fas_forcing(const Batch& fine, const Batch& coarse, const double* Rf, double* Pc, cudaStream_t s) {
+  if (coarse.ntiles) k_fas_forcing<<<coarse.ntiles, 256, 0, s>>>(fine, coarse, Rf, Pc);
+}
+void launch_fas_prolong(const Batch& fine, const Batch& coarse, double* Uf, const double* Uc, const double* Uc0,
+                        cudaStream_t s) {
+  if (fine.ntiles) k_fas_prolong<<<fine.ntiles, 256, 0, s>>>(fine, coarse, Uf, Uc, Uc0);
 }
 
 }  // namespace a2d

@@ -16,4 +16,12 @@ void launch_rk_res(const Batch& b, const double* U0, const double* U, const doub
 void launch_rk_finish(const Batch& b, const double* tpart, const double* coef, double* res, double* circ,
                       cudaStream_t s);
 
+// FAS multigrid transfers between a batch and its coarse batch (same cases, ni/2 x nc/2)
+void launch_add_forcing(const Batch& b, double* R, const double* P, cudaStream_t s);
+void launch_fas_restrict(const Batch& fine, const Batch& coarse, const double* Uf, double* Uc, double* Uc0,
+                         cudaStream_t s);
+void launch_fas_forcing(const Batch& fine, const Batch& coarse, const double* Rf, double* Pc, cudaStream_t s);
+void launch_fas_prolong(const Batch& fine, const Batch& coarse, double* Uf, const double* Uc, const double* Uc0,
+                        cudaStream_t s);
+
 }  // namespace a2d

@@ -95,6 +95,7 @@ struct a2d_plan {
   int* host_count = nullptr;
   int steps_taken = 0;
   int kernels_per_step = 0;
+  a2d_plan* coarse = nullptr;   // FAS multigrid: the same cases on grids of every other node
 
   template <typename X> X* at(size_t off) const { return reinterpret_cast<X*>(ws + off); }
   double* vec(int s) const { return at<double>(o_vec[s]); }
@@ -1160,10 +1161,30 @@ int a2d_smooth(a2d_plan* P, void* stream) {
   return A2D_OK;
 }
 
-int a2d_rk_iterate(a2d_plan* P, int n, double* res, void* stream) {
-  A2D_BOUND(P);
-  if (n < 0) return fail(A2D_ERR_ARG, "negative iteration count");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
+int a2d_plan_set_coarse(a2d_plan* P, a2d_plan* coarse) {
+  if (P == nullptr) return fail(A2D_ERR_ARG, "null plan");
+  if (coarse != nullptr) {
+    if (coarse == P || coarse->ncases != P->ncases) return fail(A2D_ERR_ARG, "set_coarse: not the same cases");
+    for (int k = 0; k < P->ncases; ++k) {
+      const GridDev& f = P->cases[k].g;
+      const GridDev& c = coarse->cases[k].g;
+      if (f.ni % 2 || f.nc % 2 || c.ni * 2 != f.ni || c.nc * 2 != f.nc)
+        return fail(A2D_ERR_ARG, "set_coarse: the coarse grids must have ni/2 x nc/2 cells (even ni, nc)");
+    }
+    for (const a2d_plan* q = coarse; q != nullptr; q = q->coarse)
+      if (q == P) return fail(A2D_ERR_ARG, "set_coarse: the levels would form a cycle");
+  }
+  P->coarse = coarse;
+  return A2D_OK;
+}
+
+}  // extern "C"
+
+namespace a2d {
+
+// one 4-stage RK iteration of plan P (aero2d/euler.py:334-346): residual at the
+// circulation circ (per case), plus the FAS forcing when given, smoothed, stage update
+static void rk_iter(a2d_plan* P, const double* circ, const double* forcing, cudaStream_t s) {
   Batch B = P->batch;
   B.live = nullptr;
   double* U = P->vec(kU);
@@ -1171,27 +1192,76 @@ int a2d_rk_iterate(a2d_plan* P, int n, double* res, void* stream) {
   double* R = P->vec(kR);
   double* Rs = P->vec(kPA);
   double* dt = P->at<double>(P->o_dt);
+  const double alphas[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
+  cudaMemcpyAsync(U0, U, 8 * 4 * (size_t)P->C, cudaMemcpyDeviceToDevice, s);
+  launch_local_dt(B, U, dt, P->p.cfl, s);
+  for (int st = 0; st < 4; ++st) {
+    StencilArgs<double> a = residual_args(P);
+    a.circ_in = circ;
+    a.out = R;
+    a.sign = 1.0;
+    launch_stencil<double, false, double>(B, a, s);
+    if (forcing != nullptr) launch_add_forcing(B, R, forcing, s);
+    const double* Ruse = R;
+    if (P->p.irs_eps > 0) {
+      launch_irs(B, R, Rs, P->p.irs_eps, P->max_ni, P->max_nc, s);
+      Ruse = Rs;
+    }
+    launch_rk_stage(B, U0, Ruse, dt, U, alphas[st], s);
+  }
+}
+
+// one FAS V-cycle from plan P down (aero2d/euler.py:368-381); at the top level
+// the pseudo-time residual of the first iteration goes to the tile partials
+static void fas_cycle(a2d_plan* P, const double* circ, const double* forcing, bool top, cudaStream_t s) {
+  Batch B = P->batch;
+  B.live = nullptr;
+  rk_iter(P, circ, forcing, s);
+  if (top) launch_rk_res(B, P->vec(kU0), P->vec(kU), P->at<double>(P->o_dt), P->at<double>(P->o_tpart), s);
+  a2d_plan* Cp = P->coarse;
+  if (Cp == nullptr) return;
+  Batch CB = Cp->batch;
+  CB.live = nullptr;
+  // fine residual (plus this level's forcing) at the smoothed state
+  StencilArgs<double> a = residual_args(P);
+  a.circ_in = circ;
+  a.out = P->vec(kR);
+  a.sign = 1.0;
+  launch_stencil<double, false, double>(B, a, s);
+  if (forcing != nullptr) launch_add_forcing(B, P->vec(kR), forcing, s);
+  // coarse start state Uc0 (kept in the coarse plan's JV slot) and forcing (its V slot)
+  double* Uc = Cp->vec(kU);
+  double* Uc0 = Cp->vec(kJV);
+  double* Pc = Cp->vec(kVin);
+  launch_fas_restrict(B, CB, P->vec(kU), Uc, Uc0, s);
+  StencilArgs<double> ca = residual_args(Cp);
+  ca.circ_in = circ;
+  ca.out = Pc;
+  ca.sign = 1.0;
+  launch_stencil<double, false, double>(CB, ca, s);
+  launch_fas_forcing(B, CB, P->vec(kR), Pc, s);
+  fas_cycle(Cp, circ, Pc, false, s);
+  launch_fas_prolong(B, CB, P->vec(kU), Uc, Uc0, s);
+  rk_iter(P, circ, forcing, s);
+}
+
+}  // namespace a2d
+
+extern "C" {
+
+int a2d_rk_iterate(a2d_plan* P, int n, double* res, void* stream) {
+  A2D_BOUND(P);
+  if (n < 0) return fail(A2D_ERR_ARG, "negative iteration count");
+  for (const a2d_plan* q = P->coarse; q != nullptr; q = q->coarse)
+    if (q->ws == nullptr) return fail(A2D_ERR_STATE, "rk_iterate: a coarse level is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Batch B = P->batch;
+  B.live = nullptr;
   double* circ = P->at<double>(P->o_circ_rk);
   double* tpart = P->at<double>(P->o_tpart);
-  const double alphas[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
   for (int it = 0; it < n; ++it) {
-    A2D_CK(cudaMemcpyAsync(U0, U, 8 * 4 * (size_t)P->C, cudaMemcpyDeviceToDevice, s));
-    launch_local_dt(B, U, dt, P->p.cfl, s);
-    for (int st = 0; st < 4; ++st) {
-      StencilArgs<double> a = residual_args(P);
-      a.circ_in = circ;
-      a.out = R;
-      a.sign = 1.0;
-      launch_stencil<double, false, double>(B, a, s);
-      const double* Ruse = R;
-      if (P->p.irs_eps > 0) {
-        launch_irs(B, R, Rs, P->p.irs_eps, P->max_ni, P->max_nc, s);
-        Ruse = Rs;
-      }
-      launch_rk_stage(B, U0, Ruse, dt, U, alphas[st], s);
-    }
-    launch_rk_res(B, U0, U, dt, tpart, s);
-    launch_forces(B, U, P->at<double>(P->o_coef), P->at<double>(P->o_cp), P->at<long long>(P->o_cpoff), nullptr,
+    fas_cycle(P, circ, nullptr, true, s);
+    launch_forces(B, P->vec(kU), P->at<double>(P->o_coef), P->at<double>(P->o_cp), P->at<long long>(P->o_cpoff), nullptr,
                   nullptr, 0, s);
     launch_rk_finish(B, tpart, P->at<double>(P->o_coef), (it == n - 1) ? res : nullptr, circ, s);
   }

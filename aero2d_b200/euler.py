@@ -140,12 +140,17 @@ class EulerSolver:
         self.ni, self.nc = self.m_np.vol.shape
         self.cfl, self.irs_eps, self.order, self.lim_k = cfl, irs_eps, order, lim_k
         self.vortex = vortex_correction
-        if mg_levels > 1:
-            if self.ni % 2 or self.nc % 2:
-                raise ValueError("multigrid needs an even number of cells in i and j")
-            raise NotImplementedError("FAS multigrid (mg_levels > 1) is not part of this build; "
-                                      "use ImplicitEuler for production runs")
+        # FAS multigrid (experimental in the reference, unstable below M 0.6 there;
+        # ImplicitEuler is the production solver): every other node in i and j,
+        # first order (aero2d/euler.py:241-250)
+        self.coarse = None
+        if mg_levels > 1 and (self.ni % 2 or self.nc % 2):
+            raise ValueError("multigrid needs an even number of cells in i and j")
         self.device = device_of(device)
+        if mg_levels > 1:
+            cg = OGrid(np.ascontiguousarray(grid.x[::2, ::2]), np.ascontiguousarray(grid.y[::2, ::2]))
+            self.coarse = EulerSolver(cg, dtype, cfl, irs_eps, order=1, vortex_correction=vortex_correction,
+                                      mg_levels=mg_levels - 1, device=self.device)
         self.dgrid = DeviceGrid(grid, self.device)
         self._plans = {}
 
@@ -234,6 +239,12 @@ class EulerSolver:
         winf = self.freestream(machs, alphas)
         B = len(machs)
         pl = Plan([self.dgrid] * B, winf, self.params(), self.device)
+        levels = [pl]                # FAS levels, finest first, linked fine -> coarse
+        lvl = self.coarse
+        while lvl is not None:
+            levels.append(Plan([lvl.dgrid] * B, winf, lvl.params(), self.device))
+            _lib.check(pl.lib.a2d_plan_set_coarse(levels[-2].handle, levels[-1].handle))
+            lvl = lvl.coarse
         if U0 is None:
             pl.init_freestream()
         else:

@@ -220,8 +220,14 @@ int a2d_time_kernel(a2d_plan* plan, int which, int reps, float* ms, void* stream
 
 /* ---- explicit RK4 + implicit residual smoothing (aero2d/euler.py:334-346) ---- */
 /* n RK iterations of every case, each followed by circ := Cl M / 2 (euler.py:398-404);
- * res: device [ncases], the RK residual of the last iteration */
+ * res: device [ncases], the RK residual of the last iteration.  With a coarse level
+ * (a2d_plan_set_coarse) each iteration is one FAS V-cycle (euler.py:368-381) through all
+ * levels, every level bound */
 int a2d_rk_iterate(a2d_plan* plan, int n, double* res, void* stream);
+/* FAS multigrid (euler.py:241-250, 349-381): `coarse` holds the same cases, in the same
+ * order, on grids of every other node (ni/2 x nc/2 cells; its params give its order, 1 in
+ * the reference); NULL unlinks.  Levels chain: the coarse plan may have its own coarse level */
+int a2d_plan_set_coarse(a2d_plan* plan, a2d_plan* coarse);
 /* R := smooth(R) in place on the residual slot (euler.py:298-312) */
 int a2d_smooth(a2d_plan* plan, void* stream);
 /* per-case circulation slot used by a2d_rk_iterate: host array [ncases] */

@@ -247,7 +247,7 @@ class EulerModel:
     """Oracle of EulerSolver.  Grid nodes (x, y) of shape (ni, nj); cells (ni, nc)."""
 
     def __init__(self, x, y, cfl=2.5, irs_eps=0.6, order=2, vortex_correction=True,
-                 lim_k=0.02):
+                 lim_k=0.02, mg_levels=1):
         x = np.asarray(x, np.float64)
         y = np.asarray(y, np.float64)
         m = compute_metrics(x, y)
@@ -261,6 +261,14 @@ class EulerModel:
         self.ni, self.nc = m.vol.shape
         k = np.arange(self.ni)
         self.irs_den_i = 1 + 2 * irs_eps * (1 - np.cos(2 * np.pi * k / self.ni))
+        # FAS multigrid (aero2d/euler.py:241-250): every other node in i and j,
+        # first order, the reference's default lim_k
+        self.coarse = None
+        if mg_levels > 1:
+            if self.ni % 2 or self.nc % 2:
+                raise ValueError("multigrid needs an even number of cells in i and j")
+            self.coarse = EulerModel(x[::2, ::2], y[::2, ::2], cfl, irs_eps, order=1,
+                                     vortex_correction=vortex_correction, mg_levels=mg_levels - 1)
 
     def freestream(self, mach, alpha_deg):
         return freestream(mach, alpha_deg)
@@ -358,16 +366,53 @@ class EulerModel:
         cl = self.forces(U, winf)[0]
         return 0.5 * cl * np.sqrt(winf[1] ** 2 + winf[2] ** 2)
 
-    def iterate(self, U, winf, circ):
-        """One 4-stage RK iteration with local time step and IRS (aero2d/euler.py:334-346)."""
+    def iterate(self, U, winf, circ, P=None):
+        """One 4-stage RK iteration with local time step and IRS, P the FAS
+        forcing term (aero2d/euler.py:334-346)."""
         U0 = U
         W = cons_to_prim(U)
         dt = self.local_dt(W)
         for a in (0.25, 1 / 3, 0.5, 1.0):
             R, _ = self.residual(U, winf, circ)
+            if P is not None:
+                R = R + P
             R = self.smooth(R)
             U = U0 - a * (dt / self.vol)[None] * R
         res = np.sqrt(np.mean(((U[0] - U0[0]) / dt) ** 2))
+        return U, res
+
+    @staticmethod
+    def sum4(a):
+        """Sum over the four fine cells of each coarse cell (aero2d/euler.py:350-352)."""
+        return a[..., 0::2, 0::2] + a[..., 1::2, 0::2] + a[..., 0::2, 1::2] + a[..., 1::2, 1::2]
+
+    @staticmethod
+    def prolong(d):
+        """Bilinear correction, weights 3/4 and 1/4, periodic in i and held at
+        the ends in j (aero2d/euler.py:354-366)."""
+        e = 0.75 * d + 0.25 * np.roll(d, 1, axis=1)
+        o = 0.75 * d + 0.25 * np.roll(d, -1, axis=1)
+        d = np.stack([e, o], axis=2).reshape(d.shape[0], -1, d.shape[2])
+        dm = np.concatenate([d[:, :, :1], d[:, :, :-1]], axis=2)
+        dp = np.concatenate([d[:, :, 1:], d[:, :, -1:]], axis=2)
+        e = 0.75 * d + 0.25 * dm
+        o = 0.75 * d + 0.25 * dp
+        return np.stack([e, o], axis=3).reshape(d.shape[0], d.shape[1], -1)
+
+    def cycle(self, U, winf, circ, P=None):
+        """One FAS V-cycle (aero2d/euler.py:368-381); without a coarse level, one iteration."""
+        U, res = self.iterate(U, winf, circ, P)
+        if self.coarse is not None:
+            cs = self.coarse
+            R, _ = self.residual(U, winf, circ)
+            if P is not None:
+                R = R + P
+            Uc0 = self.sum4(U * self.vol[None]) / self.sum4(self.vol)[None]
+            Rc, _ = cs.residual(Uc0, winf, circ)
+            Pc = self.sum4(R) - Rc
+            Uc, _ = cs.cycle(Uc0, winf, circ, Pc)
+            U = U + self.prolong(Uc - Uc0)
+            U, _ = self.iterate(U, winf, circ, P)
         return U, res
 
     def solve(self, machs, alphas, n_iter=4000, chunk=200, tol=1e-7, U0=None,
@@ -387,7 +432,7 @@ class EulerModel:
             res = np.zeros(B)
             for b in range(B):
                 for _ in range(chunk):
-                    U[b], r = self.iterate(U[b], winf[b], circ[b])
+                    U[b], r = self.cycle(U[b], winf[b], circ[b])
                     circ[b] = self.circulation(U[b], winf[b])
                 res[b] = r
             iterations = it + chunk

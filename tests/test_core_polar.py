@@ -33,6 +33,14 @@ def test_euler_grid_rejects_other_resolutions():
         euler_grid("0012", "extra fine")
 
 
+def test_multigrid_odd_grid_rejected_before_any_device_work():
+    """aero2d/euler.py:245-246."""
+    from aero2d_b200.euler import EulerSolver
+    from aero2d_b200.grid import ogrid
+    with pytest.raises(ValueError):
+        EulerSolver(ogrid(naca4("0012", 33), nj=26), dtype=np.float64, mg_levels=2)
+
+
 def test_low_mach_rejected_before_any_device_work():
     with pytest.raises(ValueError):
         run_euler("0012", [0.0, 2.0], 0.15)

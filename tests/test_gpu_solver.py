@@ -120,3 +120,19 @@ def test_nan_case_is_isolated(cuda):
     r_alone = ImplicitEuler(base, gmres_restart=20).solve([0.5], [1.0], n_iter=15, tol=1e-8, verbose=False)
     assert s.frozen[1] and not r.converged[1]
     assert torch.equal(r.U[0], r_alone.U[0])
+
+
+@pytest.mark.parametrize("levels", [2, 3])
+def test_fas_multigrid_vs_oracle(cuda, levels):
+    """FAS V-cycles (aero2d/euler.py:349-381) through every level on the device
+    against the oracle's cycles: state within 1e-9 of its change, Cl 1e-10."""
+    g = grid("0012", 33, 25)
+    om = EulerModel(g.x, g.y, mg_levels=levels)
+    ro = om.solve([0.7], [1.5], n_iter=6, chunk=3, tol=0.0)
+    s = EulerSolver(g, dtype=np.float64, device=cuda, mg_levels=levels)
+    rg = s.solve([0.7], [1.5], n_iter=6, chunk=3, tol=0.0, verbose=False)
+    U = rg.U[0].cpu().numpy()
+    dU = ro["U"][0] - om.init_state(om.freestream(0.7, 1.5))
+    assert np.max(np.abs(U - ro["U"][0])) / np.max(np.abs(dU)) < 1e-9
+    assert abs(rg.cl[0] - ro["cl"][0]) < 1e-10
+    assert np.allclose(rg.res_hist[:, 0], ro["res_hist"][:, 0], rtol=1e-9, atol=0)

@@ -122,3 +122,37 @@ def test_full_oracle_solve_reproduces_results_json(known_answers):
     assert abs(r["cl"][0] - ref["cases"][0]["cl_fp64"]) < 1e-10
     drop = np.log10(r["res_hist"][-1][0] / r["res_hist"][0][0])
     assert abs(drop - ref["log10_res_drop_fp64"][0]) < 0.2
+
+
+def test_fas_cycle_fixed_point_at_converged_state(converged_0012, known_answers):
+    """The FAS V-cycle (aero2d/euler.py:368-381) leaves a converged solution in
+    place: the coarse forcing makes the coarse problem's solution the restricted
+    state, so the prolonged correction vanishes to the residual level.  No test
+    of the reference covers its multigrid; this pins the transfers' consistency
+    (restriction, forcing and prolongation of the oracle's restatement)."""
+    g = grid("0012", 65, 49, 2e-3, 40.0)
+    ref = known_answers["results_json"]["cases"][0]
+    U = converged_0012["U_m05_a2"]
+    for levels in (2, 3):
+        m = EulerModel(g.x, g.y, mg_levels=levels)
+        w = m.freestream(ref["mach"], ref["alpha"])
+        circ = m.circulation(U, w)
+        U1, res = m.cycle(U, w, circ)
+        assert np.max(np.abs(U1 - U)) < 1e-10 * np.max(np.abs(U))
+        assert res < 1e-10
+
+
+def test_fas_transfers():
+    """Restriction preserves the volume integral; prolongation of a constant
+    correction is that constant; odd grids are rejected (aero2d/euler.py:245-246)."""
+    g = grid("2412", 33, 25)
+    m = EulerModel(g.x, g.y, mg_levels=2)
+    rng = np.random.default_rng(3)
+    U = rng.standard_normal((4, m.ni, m.nc))
+    Uc = m.sum4(U * m.vol[None]) / m.sum4(m.vol)[None]
+    assert np.allclose((Uc * m.sum4(m.vol)[None]).sum(axis=(1, 2)), (U * m.vol[None]).sum(axis=(1, 2)))
+    d = np.full((4, m.coarse.ni, m.coarse.nc), 0.37)
+    assert np.array_equal(m.prolong(d), np.full((4, m.ni, m.nc), 0.37))
+    g_odd = grid("0012", 33, 26)
+    with pytest.raises(ValueError):
+        EulerModel(g_odd.x, g_odd.y, mg_levels=2)
