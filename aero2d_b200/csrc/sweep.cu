@@ -89,7 +89,6 @@ struct SweepSmem {
   alignas(16) TC xk[kLanes][4];           // the twist row's solution
   uint64_t full[2][kS];
   uint64_t empty[2][kS];
-  int abort[2][2];                        // per half: wait failures, by step parity
   int failed[2];                          // per half: stopped early
 };
 
@@ -119,6 +118,21 @@ __device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
 // consumer threads (id 3); the producer warp takes part in none
 __device__ __forceinline__ void half_sync(int h) {
   asm volatile("bar.sync %0, %1;" ::"r"(1 + h), "r"(kHalfThreads) : "memory");
+}
+// the same barrier of one half, OR-reducing a per-thread flag over its 128 threads
+__device__ __forceinline__ bool half_sync_or(int h, bool flag) {
+  uint32_t r;
+  asm volatile(
+      "{\n"
+      " .reg .pred pi, po;\n"
+      " setp.ne.u32 pi, %1, 0;\n"
+      " bar.red.or.pred po, %2, %3, pi;\n"
+      " selp.u32 %0, 1, 0, po;\n"
+      "}\n"
+      : "=r"(r)
+      : "r"((uint32_t)flag), "r"(1 + h), "r"(kHalfThreads)
+      : "memory");
+  return r != 0;
 }
 __device__ __forceinline__ void consumers_sync() {
   asm volatile("bar.sync 3, %0;" ::"r"(kConsumerThreads) : "memory");
@@ -164,7 +178,6 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
         mbar_init(&sm.full[h][s], 1);        // the producer's arrival with the bulk-copy bytes
         mbar_init(&sm.empty[h][s], 4);       // one arrival per consumer warp of the half
       }
-      sm.abort[h][0] = sm.abort[h][1] = 0;
       sm.failed[h] = 0;
     }
     mbar_init_fence();
@@ -251,31 +264,36 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   const TC* xpv = reinterpret_cast<const TC*>(a.xprev) + vq;
   const double* rv = a.r + vq;
 
-  // the vector entries of step u (forward steps and the twist row): each thread
-  // loads component q of its line (r, or e0 and x' of both neighbour lines)
-  // into register slot sl and later stores it into the step's parity slot
+  // rows as offsets into a component plane: forward step t of the half is row
+  // jf0 + t * jdir (the wall half's twist row k continues the sequence); the
+  // back substitution runs outward from the twist row
+  const long long rstep = h == 0 ? (long long)ni : -(long long)ni;
+  const long long rf0 = h == 0 ? 0 : (long long)(nc - 1) * ni;
+  const int nvec = h == 0 ? k + 1 : nf1;       // steps with vector entries (forward, and the twist)
+
+  // the vector entries of step u: each thread loads component q of its line (r,
+  // or e0 and x' of both neighbour lines) into register slot sl and later stores
+  // it into the step's parity slot
   constexpr int L = SweepTypes<TI>::kAhead;
   double rr[L];
   TC re[L], rm[L], rp[L];
-  auto has_vec = [&](int u) { return u < nf || (h == 0 && u == k); };
-  auto load_vec = [&](int u, int sl) {
-    if (has_vec(u)) {
-      const size_t row = (size_t)row_of(h, u) * ni;
+  auto load_vec = [&](bool has, long long off, int sl) {
+    if (has) {
       if constexpr (FIRST) {
-        rr[sl] = __ldcg(rv + row + i);
+        rr[sl] = __ldcg(rv + off + i);
       } else {
-        re[sl] = __ldcg(e0v + row + i);
-        rm[sl] = __ldcg(xpv + row + im);
-        rp[sl] = __ldcg(xpv + row + ip);
+        re[sl] = __ldcg(e0v + off + i);
+        rm[sl] = __ldcg(xpv + off + im);
+        rp[sl] = __ldcg(xpv + off + ip);
       }
     }
   };
-  auto store_vec = [&](int u, int sl) {
-    if (has_vec(u)) {
+  auto store_vec = [&](bool has, int par, int sl) {
+    if (has) {
       if constexpr (FIRST) {
-        reinterpret_cast<double*>(sm.vec[h][u & 1])[l * 4 + q] = rr[sl];
+        reinterpret_cast<double*>(sm.vec[h][par])[l * 4 + q] = rr[sl];
       } else {
-        TC* v = reinterpret_cast<TC*>(sm.vec[h][u & 1]) + l * 4 + q;
+        TC* v = reinterpret_cast<TC*>(sm.vec[h][par]) + l * 4 + q;
         v[0] = re[sl];
         v[kLanes * 4] = rm[sl];
         v[2 * kLanes * 4] = rp[sl];
@@ -283,18 +301,20 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     }
   };
 
-  // waits for stage t of the half; a wait that runs out marks the step's
-  // parity slot, which every warp of the half reads after the step's barrier
+  // waits for stage t of the half; a wait that runs out is remembered and
+  // OR-reduced over the half by the step's barrier
+  bool wfail = false;
   auto wait_full = [&](int t) {
-    if (!mbar_wait(&sm.full[h][t % S], (t / S) & 1)) sm.abort[h][t & 1] = 1;
+    if (!mbar_wait(&sm.full[h][t % S], (t / S) & 1)) wfail = true;
   };
   // this warp is done with stage t % S
   auto release = [&](int t) {
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty[h][t % S]);
   };
-  // e_j of step t from the forward blocks of stage s and the step's vector entries
-  auto rhs = [&](int t, int s, int j) -> TC {
+  // e of step t from the forward blocks of stage s and the step's vector entries;
+  // the first sweep also keeps e (row offset off) for the later sweeps
+  auto rhs = [&](int t, int s, long long off) -> TC {
     const unsigned char* m = sm.mat[h][s];
     const unsigned char* vsb = sm.vec[h][t & 1];
     TC e;
@@ -305,7 +325,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
       e = iv[0] * rvv[0];
 #pragma unroll
       for (int c = 1; c < 4; ++c) e += iv[c] * rvv[c];
-      if (a.e0 != nullptr && owner) reinterpret_cast<TC*>(a.e0)[vq + (size_t)j * ni + i] = e;
+      if (a.e0 != nullptr && owner) reinterpret_cast<TC*>(a.e0)[vq + off + i] = e;
     } else {
       const TC* vs = reinterpret_cast<const TC*>(vsb);
       TC pv[4], qv[4], xm[4], xp[4];
@@ -326,13 +346,18 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   };
 
   // step 0's entries stored, steps 1 .. L in flight
-  load_vec(0, 0);
-  store_vec(0, 0);
+  long long voff = rf0;   // row of the latest vector load
+  load_vec(0 < nvec, voff, 0);
+  store_vec(0 < nvec, 0, 0);
 #pragma unroll
-  for (int u = 1; u <= L; ++u) load_vec(u, u % L);
+  for (int u = 1; u <= L; ++u) {
+    voff += rstep;
+    load_vec(u < nvec, voff, u % L);
+  }
   half_sync(h);
 
   int tstop = -1;     // step at which a wait ran out
+  long long roff = rf0;   // row of the current forward step
   // ---- forward eliminations of both halves (unrolled by L: register slots are static) ----
 #pragma unroll 1
   for (int tb = 0; tb < nf && tstop < 0; tb += L) {
@@ -341,9 +366,8 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
       const int t = tb + uu;
       if (t < nf && tstop < 0) {
         const int s = t % S;
-        const int j = row_of(h, t);
         wait_full(t);
-        const TC e = rhs(t, s, j);
+        const TC e = rhs(t, s, roff);
         TC gv[4], dp[4];
         load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
         release(t);
@@ -352,11 +376,12 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
 #pragma unroll
         for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
         sm.xchg[h][t & 1][l][q] = d;
-        if (owner) dv[(size_t)j * ni + i] = d;
-        store_vec(t + 1, (uu + 1) % L);      // step t+1's entries, published by the barrier
-        load_vec(t + 1 + L, (uu + 1) % L);   // and the slot refilled L steps ahead
-        half_sync(h);
-        if (sm.abort[h][t & 1]) tstop = t;
+        if (owner) dv[roff + i] = d;
+        roff += rstep;
+        store_vec(t + 1 < nvec, (t + 1) & 1, (uu + 1) % L);   // step t+1's entries, published by the barrier
+        voff += rstep;
+        load_vec(t + 1 + L < nvec, voff, (uu + 1) % L);       // and the slot refilled L steps ahead
+        if (half_sync_or(h, wfail)) tstop = t;
       }
     }
   }
@@ -366,8 +391,9 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   if (!(sm.failed[0] || sm.failed[1]) && h == 0) {
     const int t = k;
     const int s = t % S;
+    const long long koff = (long long)k * ni;
     wait_full(t);
-    const TC e = rhs(t, s, k);
+    const TC e = rhs(t, s, koff);
     TC gv[4], hv[4], dm[4], dpl[4];
     load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
     load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffH) + eo, hv);
@@ -381,9 +407,8 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
 #pragma unroll
     for (int c = 0; c < 4; ++c) xv += hv[c] * dpl[c];
     sm.xk[l][q] = xv;
-    if (owner) x[(size_t)k * ni + i] = TX(xv);
-    half_sync(h);
-    if (sm.abort[h][t & 1]) {
+    if (owner) x[koff + i] = TX(xv);
+    if (half_sync_or(h, wfail)) {
       tstop = t;
       if (l == 0 && q == 0) sm.failed[h] = 1;
     }
@@ -392,11 +417,14 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   // ---- back substitutions of both halves, outward from the twist row ----
   const int t0 = h == 0 ? k + 1 : nf;
   if (!(sm.failed[0] || sm.failed[1])) {
+    const long long bstep = -rstep;                               // outward from the twist row
+    long long boff = (long long)(h == 0 ? k - 1 : k + 1) * ni;    // row of back step t0
+    long long poff = boff;                                        // row of the next prefetch
     TC dbuf[kBackAhead];
 #pragma unroll
     for (int u = 0; u < kBackAhead; ++u) {
-      const int t = t0 + u;
-      dbuf[u] = t < nsteps ? dv[(size_t)row_of(h, t) * ni + i] : TC(0);
+      dbuf[u] = t0 + u < nsteps ? dv[poff + i] : TC(0);
+      poff += bstep;
     }
 #pragma unroll 1
     for (int b0 = t0; b0 < nsteps && tstop < 0; b0 += kBackAhead) {
@@ -404,7 +432,6 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
       for (int u = 0; u < kBackAhead; ++u) {
         const int t = b0 + u;
         if (t < nsteps && tstop < 0) {
-          const int j = row_of(h, t);
           const int s = t % S;
           wait_full(t);
           TC cv[4], xn[4];
@@ -416,11 +443,11 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
           for (int c = 1; c < 4; ++c) acc += cv[c] * xn[c];
           const TC xv = dbuf[u] - acc;
           sm.xchg[h][t & 1][l][q] = xv;
-          if (owner) x[(size_t)j * ni + i] = TX(xv);
-          const int tn = t + kBackAhead;
-          if (tn < nsteps) dbuf[u] = dv[(size_t)row_of(h, tn) * ni + i];
-          half_sync(h);
-          if (sm.abort[h][t & 1]) tstop = t;
+          if (owner) x[boff + i] = TX(xv);
+          boff += bstep;
+          if (t + kBackAhead < nsteps) dbuf[u] = dv[poff + i];
+          poff += bstep;
+          if (half_sync_or(h, wfail)) tstop = t;
         }
       }
     }
