@@ -129,3 +129,33 @@ def run_euler(af, alphas, mach: float, grid: str = "грубая (быстро)"
     return Polar(f"{name}, Euler ({GRID_ALIASES.get(grid, grid).split(' ')[0]}), M={mach:g}", "euler", float(mach),
                  alphas, np.asarray(cl), np.asarray(cd), np.asarray(cm), ok, [xw] * len(alphas),
                  [np.asarray(c) for c in cp], notes, nsteps=np.asarray(nsteps))
+
+
+def critical_cp(mach: float, gamma: float = 1.4) -> float:
+    """Pressure coefficient at which the local flow is sonic (isentropic)."""
+    m2 = mach * mach
+    return 2.0 / (gamma * m2) * (((2.0 + (gamma - 1.0) * m2) / (gamma + 1.0)) ** (gamma / (gamma - 1.0)) - 1.0)
+
+
+def shock_position(xw, yw, cp, mach: float) -> float:
+    """Chordwise position of the upper-surface shock: where the wall Cp (at the
+    wall-face midpoints xw, yw) rises through the critical Cp* going aft, at the
+    crossing with the steepest dCp/dx, linearly interpolated; NaN if the flow on
+    the upper surface never turns supersonic.  The reference defines no shock
+    position; this is the measure the transonic comparisons of mixed against
+    FP64 solutions use."""
+    xw, yw, cp = (np.asarray(a, float) for a in (xw, yw, cp))
+    le = int(np.argmin(xw))
+    a, b = np.arange(0, le + 1), np.arange(le, len(xw))
+    upper = a if yw[a].mean() > yw[b].mean() else b
+    order = upper[np.argsort(xw[upper])]
+    x, c = xw[order], cp[order]
+    cs = critical_cp(mach)
+    best, best_slope = float("nan"), 0.0
+    for q in range(len(x) - 1):
+        if c[q] < cs <= c[q + 1] and x[q + 1] > x[q]:
+            slope = (c[q + 1] - c[q]) / (x[q + 1] - x[q])
+            if slope > best_slope:
+                best_slope = slope
+                best = x[q] + (cs - c[q]) / (c[q + 1] - c[q]) * (x[q + 1] - x[q])
+    return best

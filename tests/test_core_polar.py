@@ -76,3 +76,16 @@ def test_service_slot_budget_on_host():
     _lib.check(lib.a2d_service_pending(h, C.byref(q), C.byref(r)))
     assert (q.value, r.value) == (1, 0)
     _lib.check(lib.a2d_service_destroy(h))
+
+
+def test_shock_position_of_a_synthetic_distribution():
+    from aero2d_b200.core import critical_cp, shock_position
+    assert abs(critical_cp(1.0)) < 1e-15 and critical_cp(0.8) < 0
+    # upper surface y > 0 from the trailing edge to the leading edge, lower back
+    x = np.concatenate([np.linspace(1, 0, 41), np.linspace(0, 1, 41)[1:]])
+    y = np.concatenate([np.full(41, 0.05), np.full(40, -0.05)])
+    cs = critical_cp(0.8)
+    cp = np.where(y > 0, np.where(x < 0.6, cs - 0.4, cs + 0.3), 0.0)
+    xs = shock_position(x, y, cp, 0.8)
+    assert 0.575 < xs < 0.6
+    assert np.isnan(shock_position(x, y, np.zeros_like(x), 0.8))
