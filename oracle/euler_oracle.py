@@ -1,7 +1,6 @@
 """CPU FP64 oracle for the Euler residual path of aero2d (reference: aero2d/euler.py).
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker that the CUDA path is
-compared against; only tests/, __graft_entry__.smoke() and bench.py's CPU
+TEST INFRASTRUCTURE ONLY.  The CUDA path is compared against this module; only tests/, __graft_entry__.smoke() and bench.py's CPU
 baseline leg may import it.  The product (aero2d_b200) never calls it.
 
 It restates, in NumPy, the arithmetic of aero2d/euler.py step by step, keeping

@@ -1,8 +1,8 @@
 """CPU FP64 oracle for the pseudo-transient Newton-Krylov solver of aero2d
 (reference: aero2d/implicit.py).
 
-TEST INFRASTRUCTURE ONLY (see oracle/euler_oracle.py): the checker for the
-CUDA path, never part of the product.
+TEST INFRASTRUCTURE ONLY (see oracle/euler_oracle.py): what the CUDA path is
+compared against, never part of the product.
 
 Derivatives that the reference takes with jax.jvp / jax.jacfwd are taken here
 by the complex step on the oracle residual, which is exact to rounding.

@@ -37,5 +37,5 @@ def cuda():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     from aero2d_b200 import _lib
-    _lib.load()          # a GPU box without the built library must fail, not skip
+    _lib.load()          # a GPU machine without the built library must fail, not skip
     return torch.device("cuda", 0)
