@@ -64,22 +64,26 @@ constexpr int kVB = 256;                 // threads per vector block
 constexpr int kPer = kChunk / kVB;       // entries per thread
 
 // ---------------------------------------------------------------------------
-// Hessenberg least squares min || beta e1 - H y || by Givens rotations, one
-// thread per case (H column k = Arnoldi step k)
+// Hessenberg least squares min || beta e1 - H y || by Givens rotations (H
+// column k = Arnoldi step k).  One warp per case copies the case's columns
+// into shared memory; its first lane then rotates and back-substitutes there
+// (a sequential chain of dependent updates: in shared memory each costs a few
+// tens of cycles instead of a global-memory round trip).
 // ---------------------------------------------------------------------------
-__global__ void k_lstsq(int ncases, const uint32_t* live, CaseCtl* ctl, double* Hall, double* yall,
-                        double* scr) {
-  const int cs = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cs >= ncases) return;
+__global__ void __launch_bounds__(32) k_lstsq(int ncases, const uint32_t* live, CaseCtl* ctl, const double* Hall,
+                                              double* yall) {
+  const int cs = blockIdx.x;
   if (!(live[cs] & kLiveNewton)) return;
   const int k = ctl[cs].k_used;
-  double* y = yall + (size_t)cs * kMaxRestart;
   if (k == 0) return;
   constexpr int L = kMaxRestart + 1;
-  double* Hc = Hall + (size_t)cs * kMaxRestart * L;   // column j at Hc[j * L + q]; rotated in place
-  double* g = scr + (size_t)cs * 3 * L;
-  double* cr = g + L;
-  double* sr = cr + L;
+  __shared__ double Hc[kMaxRestart * L];   // column j at Hc[j * L + q]; rotated in place
+  __shared__ double g[L], cr[L], sr[L];
+  const double* Hg = Hall + (size_t)cs * kMaxRestart * L;
+  for (int e = threadIdx.x; e < k * L; e += blockDim.x) Hc[e] = Hg[e];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double* y = yall + (size_t)cs * kMaxRestart;
   for (int q = 0; q <= k; ++q) g[q] = 0.0;
   g[0] = ctl[cs].beta;
   for (int j = 0; j < k; ++j) {
@@ -327,9 +331,8 @@ template <typename TB>
 void launch_combine(const Batch& b, const CombineArgs<TB>& a, cudaStream_t s) {
   if (b.nchunks) k_combine<TB><<<b.nchunks, kVB, 0, s>>>(b, a);
 }
-void launch_lstsq(const Batch& b, const uint32_t* live, CaseCtl* ctl, double* H, double* y, double* scr,
-                  cudaStream_t s) {
-  k_lstsq<<<(b.ncases + 31) / 32, 32, 0, s>>>(b.ncases, live, ctl, H, y, scr);
+void launch_lstsq(const Batch& b, const uint32_t* live, CaseCtl* ctl, double* H, double* y, cudaStream_t s) {
+  k_lstsq<<<b.ncases, 32, 0, s>>>(b.ncases, live, ctl, H, y);
 }
 void launch_gm_setup(const Batch& b, const double* part, int pstride, CaseCtl* ctl, double gtol,
                      cudaStream_t s) {

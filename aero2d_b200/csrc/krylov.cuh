@@ -27,8 +27,7 @@ struct CombineArgs {
 };
 
 template <typename TB> void launch_combine(const Batch& b, const CombineArgs<TB>& a, cudaStream_t s);
-void launch_lstsq(const Batch& b, const uint32_t* live, CaseCtl* ctl, double* H, double* y, double* scr,
-                  cudaStream_t s);
+void launch_lstsq(const Batch& b, const uint32_t* live, CaseCtl* ctl, double* H, double* y, cudaStream_t s);
 void launch_gm_setup(const Batch& b, const double* part, int pstride, CaseCtl* ctl, double gtol,
                      cudaStream_t s);
 void launch_norms2(const Batch& b, const double* x, const double* y, double* part, int pstride,

@@ -84,7 +84,7 @@ struct a2d_plan {
   size_t o_cases = 0, o_tiles = 0, o_chunks = 0, o_groups = 0, o_cpoff = 0, o_live = 0, o_ctl = 0;
   size_t o_vec[kNumVec] = {};
   size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_PQG = 0, o_V = 0;
-  size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_lsq = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
+  size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
   size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0, o_idx = 0;
   int pstride = 0;
   size_t bytes = 0;
@@ -176,7 +176,6 @@ static void layout(a2d_plan* P) {
   P->o_h2 = cv.take(8 * (size_t)B * kHStride);
   P->o_scale = cv.take(8 * (size_t)B * (P->m + 1));
   P->o_y = cv.take(8 * (size_t)B * kMaxRestart);
-  P->o_lsq = cv.take(8 * (size_t)B * 3 * (kMaxRestart + 1));
   P->o_wn0 = cv.take(8 * (size_t)B);
   P->o_circ = cv.take(8 * (size_t)B);
   P->o_circ_rk = cv.take(8 * (size_t)B);
@@ -507,7 +506,7 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
     ck.need = KR;
     launch_gs_close(B, ck, s);
   }
-  launch_lstsq(B, live, ctl, P->at<double>(P->o_H), P->at<double>(P->o_y), P->at<double>(P->o_lsq), s);
+  launch_lstsq(B, live, ctl, P->at<double>(P->o_H), P->at<double>(P->o_y), s);
   CombineArgs<TB> ca;
   ca.x0 = x0;
   ca.V = V;
