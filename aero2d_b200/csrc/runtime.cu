@@ -1183,7 +1183,7 @@ namespace a2d {
 
 // one 4-stage RK iteration of plan P (aero2d/euler.py:334-346): residual at the
 // circulation circ (per case), plus the FAS forcing when given, smoothed, stage update
-static void rk_iter(a2d_plan* P, const double* circ, const double* forcing, cudaStream_t s) {
+static cudaError_t rk_iter(a2d_plan* P, const double* circ, const double* forcing, cudaStream_t s) {
   Batch B = P->batch;
   B.live = nullptr;
   double* U = P->vec(kU);
@@ -1192,7 +1192,7 @@ static void rk_iter(a2d_plan* P, const double* circ, const double* forcing, cuda
   double* Rs = P->vec(kPA);
   double* dt = P->at<double>(P->o_dt);
   const double alphas[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
-  cudaMemcpyAsync(U0, U, 8 * 4 * (size_t)P->C, cudaMemcpyDeviceToDevice, s);
+  if (cudaError_t e = cudaMemcpyAsync(U0, U, 8 * 4 * (size_t)P->C, cudaMemcpyDeviceToDevice, s)) return e;
   launch_local_dt(B, U, dt, P->p.cfl, s);
   for (int st = 0; st < 4; ++st) {
     StencilArgs<double> a = residual_args(P);
@@ -1208,17 +1208,18 @@ static void rk_iter(a2d_plan* P, const double* circ, const double* forcing, cuda
     }
     launch_rk_stage(B, U0, Ruse, dt, U, alphas[st], s);
   }
+  return cudaGetLastError();
 }
 
 // one FAS V-cycle from plan P down (aero2d/euler.py:368-381); at the top level
 // the pseudo-time residual of the first iteration goes to the tile partials
-static void fas_cycle(a2d_plan* P, const double* circ, const double* forcing, bool top, cudaStream_t s) {
+static cudaError_t fas_cycle(a2d_plan* P, const double* circ, const double* forcing, bool top, cudaStream_t s) {
   Batch B = P->batch;
   B.live = nullptr;
-  rk_iter(P, circ, forcing, s);
+  if (cudaError_t e = rk_iter(P, circ, forcing, s)) return e;
   if (top) launch_rk_res(B, P->vec(kU0), P->vec(kU), P->at<double>(P->o_dt), P->at<double>(P->o_tpart), s);
   a2d_plan* Cp = P->coarse;
-  if (Cp == nullptr) return;
+  if (Cp == nullptr) return cudaGetLastError();
   Batch CB = Cp->batch;
   CB.live = nullptr;
   // fine residual (plus this level's forcing) at the smoothed state
@@ -1239,9 +1240,9 @@ static void fas_cycle(a2d_plan* P, const double* circ, const double* forcing, bo
   ca.sign = 1.0;
   launch_stencil<double, false, double>(CB, ca, s);
   launch_fas_forcing(B, CB, P->vec(kR), Pc, s);
-  fas_cycle(Cp, circ, Pc, false, s);
+  if (cudaError_t e = fas_cycle(Cp, circ, Pc, false, s)) return e;
   launch_fas_prolong(B, CB, P->vec(kU), Uc, Uc0, s);
-  rk_iter(P, circ, forcing, s);
+  return rk_iter(P, circ, forcing, s);
 }
 
 }  // namespace a2d
@@ -1259,7 +1260,7 @@ int a2d_rk_iterate(a2d_plan* P, int n, double* res, void* stream) {
   double* circ = P->at<double>(P->o_circ_rk);
   double* tpart = P->at<double>(P->o_tpart);
   for (int it = 0; it < n; ++it) {
-    fas_cycle(P, circ, nullptr, true, s);
+    A2D_CK(fas_cycle(P, circ, nullptr, true, s));
     launch_forces(B, P->vec(kU), P->at<double>(P->o_coef), P->at<double>(P->o_cp), P->at<long long>(P->o_cpoff), nullptr,
                   nullptr, 0, s);
     launch_rk_finish(B, tpart, P->at<double>(P->o_coef), (it == n - 1) ? res : nullptr, circ, s);

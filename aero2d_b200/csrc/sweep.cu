@@ -267,8 +267,15 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   // rows as offsets into a component plane: forward step t of the half is row
   // jf0 + t * jdir (the wall half's twist row k continues the sequence); the
   // back substitution runs outward from the twist row
-  const long long rstep = h == 0 ? (long long)ni : -(long long)ni;
-  const long long rf0 = h == 0 ? 0 : (long long)(nc - 1) * ni;
+  const int rstep = h == 0 ? ni : -ni;
+  const int rf0 = h == 0 ? 0 : (nc - 1) * ni;
+  // per-thread bases: offsets within a component plane stay 32-bit
+  const TC* e0b = e0v + i;
+  const TC* xmb = xpv + im;
+  const TC* xpb = xpv + ip;
+  const double* rb = rv + i;
+  TC* dvb = dv + i;
+  TX* xb = x + i;
   const int nvec = h == 0 ? k + 1 : nf1;       // steps with vector entries (forward, and the twist)
 
   // the vector entries of step u: each thread loads component q of its line (r,
@@ -277,14 +284,14 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   constexpr int L = SweepTypes<TI>::kAhead;
   double rr[L];
   TC re[L], rm[L], rp[L];
-  auto load_vec = [&](bool has, long long off, int sl) {
+  auto load_vec = [&](bool has, int off, int sl) {
     if (has) {
       if constexpr (FIRST) {
-        rr[sl] = __ldcg(rv + off + i);
+        rr[sl] = __ldcg(rb + off);
       } else {
-        re[sl] = __ldcg(e0v + off + i);
-        rm[sl] = __ldcg(xpv + off + im);
-        rp[sl] = __ldcg(xpv + off + ip);
+        re[sl] = __ldcg(e0b + off);
+        rm[sl] = __ldcg(xmb + off);
+        rp[sl] = __ldcg(xpb + off);
       }
     }
   };
@@ -314,7 +321,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   };
   // e of step t from the forward blocks of stage s and the step's vector entries;
   // the first sweep also keeps e (row offset off) for the later sweeps
-  auto rhs = [&](int t, int s, long long off) -> TC {
+  auto rhs = [&](int t, int s, int off) -> TC {
     const unsigned char* m = sm.mat[h][s];
     const unsigned char* vsb = sm.vec[h][t & 1];
     TC e;
@@ -325,7 +332,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
       e = iv[0] * rvv[0];
 #pragma unroll
       for (int c = 1; c < 4; ++c) e += iv[c] * rvv[c];
-      if (a.e0 != nullptr && owner) reinterpret_cast<TC*>(a.e0)[vq + off + i] = e;
+      if (a.e0 != nullptr && owner) reinterpret_cast<TC*>(a.e0)[vq + i + off] = e;
     } else {
       const TC* vs = reinterpret_cast<const TC*>(vsb);
       TC pv[4], qv[4], xm[4], xp[4];
@@ -346,7 +353,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   };
 
   // step 0's entries stored, steps 1 .. L in flight
-  long long voff = rf0;   // row of the latest vector load
+  int voff = rf0;   // row of the latest vector load
   load_vec(0 < nvec, voff, 0);
   store_vec(0 < nvec, 0, 0);
 #pragma unroll
@@ -357,7 +364,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   half_sync(h);
 
   int tstop = -1;     // step at which a wait ran out
-  long long roff = rf0;   // row of the current forward step
+  int roff = rf0;   // row of the current forward step
   // ---- forward eliminations of both halves (unrolled by L: register slots are static) ----
 #pragma unroll 1
   for (int tb = 0; tb < nf && tstop < 0; tb += L) {
@@ -376,7 +383,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
 #pragma unroll
         for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
         sm.xchg[h][t & 1][l][q] = d;
-        if (owner) dv[roff + i] = d;
+        if (owner) dvb[roff] = d;
         roff += rstep;
         store_vec(t + 1 < nvec, (t + 1) & 1, (uu + 1) % L);   // step t+1's entries, published by the barrier
         voff += rstep;
@@ -391,7 +398,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   if (!(sm.failed[0] || sm.failed[1]) && h == 0) {
     const int t = k;
     const int s = t % S;
-    const long long koff = (long long)k * ni;
+    const int koff = k * ni;
     wait_full(t);
     const TC e = rhs(t, s, koff);
     TC gv[4], hv[4], dm[4], dpl[4];
@@ -407,7 +414,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
 #pragma unroll
     for (int c = 0; c < 4; ++c) xv += hv[c] * dpl[c];
     sm.xk[l][q] = xv;
-    if (owner) x[koff + i] = TX(xv);
+    if (owner) xb[koff] = TX(xv);
     if (half_sync_or(h, wfail)) {
       tstop = t;
       if (l == 0 && q == 0) sm.failed[h] = 1;
@@ -417,13 +424,13 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   // ---- back substitutions of both halves, outward from the twist row ----
   const int t0 = h == 0 ? k + 1 : nf;
   if (!(sm.failed[0] || sm.failed[1])) {
-    const long long bstep = -rstep;                               // outward from the twist row
-    long long boff = (long long)(h == 0 ? k - 1 : k + 1) * ni;    // row of back step t0
-    long long poff = boff;                                        // row of the next prefetch
+    const int bstep = -rstep;                               // outward from the twist row
+    int boff = (h == 0 ? k - 1 : k + 1) * ni;               // row of back step t0
+    int poff = boff;                                        // row of the next prefetch
     TC dbuf[kBackAhead];
 #pragma unroll
     for (int u = 0; u < kBackAhead; ++u) {
-      dbuf[u] = t0 + u < nsteps ? dv[poff + i] : TC(0);
+      dbuf[u] = t0 + u < nsteps ? dvb[poff] : TC(0);
       poff += bstep;
     }
 #pragma unroll 1
@@ -443,9 +450,9 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
           for (int c = 1; c < 4; ++c) acc += cv[c] * xn[c];
           const TC xv = dbuf[u] - acc;
           sm.xchg[h][t & 1][l][q] = xv;
-          if (owner) x[boff + i] = TX(xv);
+          if (owner) xb[boff] = TX(xv);
           boff += bstep;
-          if (t + kBackAhead < nsteps) dbuf[u] = dv[poff + i];
+          if (t + kBackAhead < nsteps) dbuf[u] = dvb[poff];
           poff += bstep;
           if (half_sync_or(h, wfail)) tstop = t;
         }
