@@ -1,21 +1,17 @@
 """Polar scenario on the Euler path: the reference's `run_euler` and its
 `Polar` record (aero2d/core.py:20-45, :220-260) on this backend.
 
-`run_euler(af, alphas, mach, grid, n_iter, callback)` solves every angle of
-attack as one batch with ImplicitEuler in FP32 (the reference's settings: tol
-1e-6, the grid levels of `GRIDS`, far field 40 chords, all angles stepped in
-lockstep until every one is done) and returns a `Polar`
-with Cl, Cd, Cm, the wall Cp at the wall-face midpoints and the per-angle
-convergence flags, with the reference's notes for unconverged angles.  With
-`continuation=True` the angles are instead solved one after another from the
-previous angle's state (alpha continuation) through EulerService.
-
-The reference re-panels any contour to the grid level's points per side with a
-spline (aero2d/geometry.py:320); that geometry routine is not part of this
-path, so `af` must already have 2 n_side - 1 points for the chosen level (as
-`naca4(code, n_side)` gives), or be a NACA 4-digit code string, which is built
-at that resolution directly (a re-panelled contour and a directly built one
-differ at the level of the spline error, ~1e-4 in Cl).
+`run_euler(af, alphas, mach, grid, n_iter, callback)` re-panels the contour to
+the grid level's points per side (geometry.repanel, as aero2d/core.py:236
+does for every input), marches the level's O-grid (far field 40 chords),
+solves every angle of attack as one batch with ImplicitEuler in FP32 (tol
+1e-6, all angles stepped in lockstep until every one is done, as the
+reference's loop does) and returns a `Polar` with Cl, Cd, Cm, the wall Cp at
+the wall-face midpoints and the per-angle convergence flags, with the
+reference's notes for unconverged angles.  With `continuation=True` the angles
+are instead solved one after another from the previous angle's state (alpha
+continuation) through EulerService.  `af` is an Airfoil or a NACA 4-digit code
+(built as naca4(code), the reference's default resolution, then re-panelled).
 """
 from __future__ import annotations
 
@@ -24,7 +20,7 @@ from typing import Optional
 
 import numpy as np
 
-from .geometry import Airfoil, naca4
+from .geometry import Airfoil, naca4, repanel
 from .grid import ogrid
 
 # grid levels: (points per side of the contour, nodes along the normal, first spacing),
@@ -66,16 +62,13 @@ def _level(grid: str) -> tuple[int, int, float]:
 
 
 def euler_grid(af, grid: str = "грубая (быстро)"):
-    """The O-grid of a grid level for an airfoil (see the module docstring)."""
+    """The re-panelled contour and O-grid of a grid level (aero2d/core.py:234-236)."""
     nside, nj, ds0 = _level(grid)
     if isinstance(af, str):
-        af = naca4(af, nside)
+        af = naca4(af)
     if not isinstance(af, Airfoil):
         raise TypeError("af must be an Airfoil or a NACA 4-digit code")
-    if len(af.x) != 2 * nside - 1:
-        raise NotImplementedError(
-            f"the contour has {len(af.x)} points; this grid level needs {2 * nside - 1} "
-            f"(re-panelling arbitrary contours, aero2d/geometry.py:320, is outside this path)")
+    af = repanel(af, nside)
     return af, ogrid(af, nj=nj, ds0=ds0, radius=FARFIELD_RADIUS)
 
 

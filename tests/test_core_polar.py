@@ -16,19 +16,24 @@ def test_grid_levels_match_the_reference_table():
 
 def test_euler_grid_from_code_and_airfoil():
     af, g = euler_grid("0012", "coarse")
-    assert g.x.shape == (128, 49)
-    af2, g2 = euler_grid(naca4("0012", 65), "грубая (быстро)")
+    assert g.x.shape == (128, 49) and len(af.x) == 129
+    af2, g2 = euler_grid(naca4("0012"), "грубая (быстро)")
     assert np.array_equal(g.x, g2.x) and np.array_equal(g.y, g2.y)
+    with pytest.raises(TypeError):
+        euler_grid(np.zeros((10, 2)), "coarse")
 
 
-def test_coarse_level_is_the_reference_benchmark_grid(ref_grids):
+def test_coarse_level_is_the_reference_polar_grid():
+    """The reference's polar grid, ogrid(repanel(naca4("0012"), 65), ...), bitwise."""
+    from tests.conftest import GOLDEN
+    d = np.load(GOLDEN / "ref_repanel.npz")
     _, g = euler_grid("0012", "coarse")
-    assert np.array_equal(g.x, ref_grids["0012_65_49_x"]) and np.array_equal(g.y, ref_grids["0012_65_49_y"])
+    assert np.array_equal(g.x, d["polar_coarse_0012_x"]) and np.array_equal(g.y, d["polar_coarse_0012_y"])
 
 
-def test_euler_grid_rejects_other_resolutions():
-    with pytest.raises(NotImplementedError):
-        euler_grid(naca4("0012", 100), "coarse")
+def test_any_contour_is_repanelled_to_the_level():
+    af, g = euler_grid(naca4("2412", 40), "medium")
+    assert len(af.x) == 2 * 97 - 1 and g.x.shape == (192, 65)
     with pytest.raises(ValueError):
         euler_grid("0012", "extra fine")
 

@@ -58,17 +58,22 @@ def test_service_continuation_takes_fewer_steps(cuda):
     svc.close()
 
 
-def test_run_euler_known_answer(cuda, known_answers):
-    """The coarse level is the reference benchmark's grid (128 x 48 cells, radius
-    40): Cl at M 0.5, alpha 2 deg (benchmarks/results.json, 0.2816252).  The
-    polar stops at the reference's 1e-6 residual drop, where Cl is measured
-    2.5e-4 short of the converged value on this grid, so the bound is 4e-4; at
-    the same drop the continued sweep agrees within that convergence error."""
+def test_run_euler_known_answer(cuda):
+    """The polar scenario re-panels the contour to the level's 65 points per side
+    before marching the 128 x 48 grid, as the reference's run_euler does; on
+    that grid the FP64 oracle gives Cl 0.2832521 at M 0.5, alpha 2 deg
+    (tests/golden/polar_known_answer.json, residual down 13 orders).  The polar
+    stops at the reference's 1e-6 drop, measured about 2.5e-4 short of the
+    converged Cl on these grids, so the bound is 4e-4; at the same drop the
+    continued sweep agrees within that convergence error."""
+    import json
+    from tests.conftest import GOLDEN
+    ref = json.load(open(GOLDEN / "polar_known_answer.json"))
     p = run_euler("0012", [0.0, 2.0], 0.5, grid="coarse", n_iter=100, device=cuda)
     assert p.ok.all()
     assert abs(p.cl[0]) < 1e-6
-    assert abs(p.cl[1] - known_answers["results_json"]["cases"][0]["cl_fp64"]) < 4e-4
-    assert len(p.cp) == 2 and p.cp[0].shape == p.cp_x[0].shape
+    assert abs(p.cl[1] - ref["cl_fp64"]) < 4e-4
+    assert len(p.cp) == 2 and p.cp[0].shape == p.cp_x[0].shape == (128,)
     pc = run_euler("0012", [0.0, 2.0], 0.5, grid="coarse", n_iter=100, continuation=True, device=cuda)
     assert pc.ok.all()
     assert np.max(np.abs(pc.cl - p.cl)) < 4e-4

@@ -98,3 +98,17 @@ def test_device_grid_spacing_matches_host(nj, ds0, radius):
     _lib.check(_lib.load().a2d_grid_spacing(nj, ds0, radius, out.ctypes.data_as(C.POINTER(C.c_double))))
     ref = layer_spacing(nj, ds0, radius)
     assert np.max(np.abs(out - ref) / ref) <= 2.3e-16
+
+
+def test_repanel_matches_reference():
+    """Arc-length spline re-panelling (aero2d/geometry.py:320-391), bitwise the
+    reference's own output on the same contours (tests/golden/ref_repanel.npz):
+    NACA sections at the polar levels' resolutions, a blunt trailing edge, a
+    contour with corners, two-halves input, a mirrored unnormalised contour and
+    the viscous spacing."""
+    from aero2d_b200.geometry import Airfoil, repanel
+    from tests.golden.make_golden import REPANEL_KW
+    d = np.load(ROOT / "tests" / "golden" / "ref_repanel.npz")
+    for key, kw in REPANEL_KW.items():
+        out = repanel(Airfoil(d[f"{key}_in_x"], d[f"{key}_in_y"]), **kw)
+        assert np.array_equal(out.x, d[f"{key}_out_x"]) and np.array_equal(out.y, d[f"{key}_out_y"]), key
