@@ -269,8 +269,23 @@ int a2d_service_step(a2d_service* S, int* busy, void* stream) {
     if (int e = a2d_case_restart(S->plan, (int)keep_k.size(), keep_k.data(), keep_w.data(), 1, stream)) return e;
   if (!fresh_k.empty())
     if (int e = a2d_case_restart(S->plan, (int)fresh_k.size(), fresh_k.data(), fresh_w.data(), 0, stream)) return e;
-  if (!retire_k.empty())
+  if (!retire_k.empty()) {
     if (int e = a2d_case_retire(S->plan, (int)retire_k.size(), retire_k.data(), stream)) return e;
+    // a freed slot goes back to its class's own grid: the finished request's grid belongs to
+    // the caller, who may free it once the result is taken, and a2d_case_forces reads every slot
+    std::vector<int> back;
+    std::vector<const void*> back_m;
+    for (int k : retire_k) {
+      const void* m = S->classes[S->slot_cls[k]].metrics;
+      if (S->slot_metrics[k] != m) {
+        S->slot_metrics[k] = m;
+        back.push_back(k);
+        back_m.push_back(m);
+      }
+    }
+    if (!back.empty())
+      if (int e = a2d_case_set_grid(S->plan, (int)back.size(), back.data(), back_m.data(), stream)) return e;
+  }
   return A2D_OK;
 }
 
