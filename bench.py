@@ -227,6 +227,17 @@ def read_traffic(kernel: str):
     return None
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux), for the CPU-baseline lines."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -397,6 +408,7 @@ def gpu_arm(args, rank: int, world: int, dist):
         procs = max(1, min(os.cpu_count() or 1, args.cpu_procs))
         rate, per_step, cpu_wall = cpu_oracle_rate(procs)
         out["cpu_baseline"] = {"value": round(rate, 5), "unit": "cases/s", "cores": procs, "kind": "port",
+                               "cpu": f"{cpu_model()}, {os.cpu_count()} logical CPUs",
                                "sample": f"one Newton step (restart {RESTART}, 4 sweeps) of {procs} cases of this "
                                          f"workload, one spawned process per case with one BLAS thread, "
                                          f"{per_step:.2f} s per step; cases/s = processes / step time / "
@@ -542,6 +554,7 @@ def reference_arm(args):
                                    f"alpha~U[-4,8] deg, seed {SEED}, Newton-Krylov to residual drop {TOL:g}",
                        "gmres_restart": RESTART},
             "cpu_baseline": {"value": round(value, 5), "unit": "cases/s", "cores": procs, "kind": "port",
+                             "cpu": f"{cpu_model()}, {os.cpu_count()} logical CPUs",
                              "sample": f"per step: one Newton step of {procs} cases on {procs} spawned processes "
                                        f"({statistics.mean(per):.2f} s per Newton step); the JAX reference "
                                        "cannot be installed in this image (no jax wheel, no network)"},
