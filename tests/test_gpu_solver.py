@@ -136,3 +136,15 @@ def test_fas_multigrid_vs_oracle(cuda, levels):
     assert np.max(np.abs(U - ro["U"][0])) / np.max(np.abs(dU)) < 1e-9
     assert abs(rg.cl[0] - ro["cl"][0]) < 1e-10
     assert np.allclose(rg.res_hist[:, 0], ro["res_hist"][:, 0], rtol=1e-9, atol=0)
+
+
+def test_explicit_nan_raises(cuda):
+    """A non-finite explicit run stops at the end of its chunk and raises
+    FloatingPointError (aero2d/euler.py:423-432)."""
+    g = grid("0012", 33, 25)
+    s = EulerSolver(g, dtype=np.float64, device=cuda)
+    w = s.freestream(np.array([0.5]), np.array([1.0]))
+    U0 = s.init_state(w)
+    U0[0, 0, 5, 3] = float("nan")
+    with pytest.raises(FloatingPointError):
+        s.solve([0.5], [1.0], n_iter=4, chunk=2, tol=0.0, verbose=False, U0=U0)
