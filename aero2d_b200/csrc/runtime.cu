@@ -22,6 +22,8 @@
 #include "batch.cuh"
 #include "explicit.cuh"
 #include "kernels.cuh"
+
+#include <nvtx3/nvToolsExt.h>
 #include "gs.cuh"
 #include "krylov.cuh"
 #include "physics.cuh"
@@ -313,6 +315,15 @@ __global__ void k_point_flux(int n, const double* WL, const double* WR, const do
 // ---------------------------------------------------------------------------
 namespace a2d {
 
+// NVTX range for profilers (no cost without one attached): the stages of a Newton
+// step when it runs without a graph, and the C ABI's solver entry points
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
+
 static SweepArgs sweep_args(const a2d_plan* P, uint32_t need) {
   SweepArgs a;
   a.INV = P->at<void>(P->o_INV);
@@ -405,6 +416,7 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
   CaseCtl* ctl = P->ctl();
   uint32_t* live = P->live();
 
+  nvtxRangePushA("newton: residual and line preconditioner");
   launch_mark_stepped(B, live, ctl, s);
   // Newton right-hand side b = -R(U) in FP64, circulation from U, residual-norm partials
   StencilArgs<double> ra = residual_args(P);
@@ -416,6 +428,8 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
   launch_stencil<double, false, double>(B, ra, s);
   // line preconditioner at U
   precond_setup<TJ>(P, B, NW, s);
+  nvtxRangePop();
+  nvtxRangePushA("newton: GMRES start");
   // x0 = M b; ptol from ||b||, ||M b||
   precond<TJ>(P, B, b, x0, NW, s);
   launch_norms2(B, b, x0, cpart, P->pstride, NW, s);
@@ -448,6 +462,8 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
   c0.k = -1;
   c0.need = NW;
   launch_gs_close(B, c0, s);
+  nvtxRangePop();
+  nvtxRangePushA("newton: Arnoldi");
   for (int k = 0; k < P->m; ++k) {
     StencilArgs<TB> za;
     za.U = U;
@@ -506,6 +522,8 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
     ck.need = KR;
     launch_gs_close(B, ck, s);
   }
+  nvtxRangePop();
+  nvtxRangePushA("newton: least squares and update");
   launch_lstsq(B, live, ctl, P->at<double>(P->o_H), P->at<double>(P->o_y), s);
   CombineArgs<TB> ca;
   ca.x0 = x0;
@@ -529,6 +547,7 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
   launch_commit(B, U, dU, ctl, s);
   launch_forces(B, U, P->at<double>(P->o_coef), P->at<double>(P->o_cp), P->at<long long>(P->o_cpoff), ctl,
                 P->at<double>(P->o_hcl), P->p.max_iter, s);
+  nvtxRangePop();
 }
 
 static void newton_dispatch(a2d_plan* P, cudaStream_t s) {
@@ -911,6 +930,7 @@ int a2d_precond_apply(a2d_plan* P, void* stream) {
 
 int a2d_newton_step(a2d_plan* P, void* stream) {
   A2D_BOUND(P);
+  Range range("a2d_newton_step");
   const int e = newton_step(P, static_cast<cudaStream_t>(stream));
   if (e == A2D_OK) P->steps_taken += 1;
   return e;
@@ -918,6 +938,7 @@ int a2d_newton_step(a2d_plan* P, void* stream) {
 
 int a2d_newton_run(a2d_plan* P, int max_steps, int* steps, void* stream) {
   A2D_BOUND(P);
+  Range range("a2d_newton_run");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int done = 0;
   int* dcount = P->at<int>(P->o_cnt);
@@ -1251,6 +1272,7 @@ extern "C" {
 
 int a2d_rk_iterate(a2d_plan* P, int n, double* res, void* stream) {
   A2D_BOUND(P);
+  Range range("a2d_rk_iterate");
   if (n < 0) return fail(A2D_ERR_ARG, "negative iteration count");
   for (const a2d_plan* q = P->coarse; q != nullptr; q = q->coarse)
     if (q->ws == nullptr) return fail(A2D_ERR_STATE, "rk_iterate: a coarse level is not bound");
