@@ -80,6 +80,8 @@ SIGNATURES = {
     "a2d_plan_ncases": (_I, [_P]),
     "a2d_vec_set": (_I, [_P, _I, _I, _P, _P]),
     "a2d_vec_get": (_I, [_P, _I, _I, _P, _P]),
+    "a2d_vec_get_prim": (_I, [_P, _I, _I, _P, _P]),
+    "a2d_local_dt": (_I, [_P, _I, _P, _P, _P]),
     "a2d_init_freestream": (_I, [_P, _P]),
     "a2d_reset": (_I, [_P, _P]),
     "a2d_residual": (_I, [_P, _P, _P]),
@@ -95,6 +97,7 @@ SIGNATURES = {
     "a2d_case_scalars": (_I, [_P, C.POINTER(_D), _P]),
     "a2d_history": (_I, [_P, _I, C.POINTER(_D), C.POINTER(_D), _P]),
     "a2d_live_count": (_I, [_P, C.POINTER(_I), _P]),
+    "a2d_factor_saturations": (_I, [_P, C.POINTER(C.c_ulonglong), _I, _P]),
     "a2d_plan_stats": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_SZ)]),
     "a2d_time_kernel": (_I, [_P, _I, _I, C.POINTER(C.c_float), _P]),
     "a2d_rk_iterate": (_I, [_P, _I, _P, _P]),

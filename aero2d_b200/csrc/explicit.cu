@@ -8,36 +8,59 @@
 // e l^2 - (1+2e) l + e = 0 and G0 = 1 / (e (1/l - l)); terms with l^|m| below
 // 1e-18 of the diagonal are dropped, so results equal the FFT's to rounding.
 // Smoothing along j is a Thomas solve of (-e, 1+2e, -e) with end diagonals 1+e.
+#include <algorithm>
+
 #include "batch.cuh"
 #include "explicit.cuh"
 #include "physics.cuh"
 
 namespace a2d {
 
-// local time step dt = cfl vol / (lambda_i + lambda_j)   (euler.py:289-296)
+// local time step of cell (j, i) from its primitives W = (rho, u, v, p):
+// dt = cfl vol / (lambda_i + lambda_j), face vectors averaged to the cell
+// centre, in the operation order of euler.py:289-296
+__device__ __forceinline__ double local_dt_cell(const GridDev& g, const State4<double>& W, int j, int i,
+                                                double cfl) {
+  const int ni = g.ni, nc = g.nc;
+  const size_t N = (size_t)ni * nc, NJ = (size_t)(nc + 1) * ni;
+  const int ip = (i + 1 == ni) ? 0 : i + 1;
+  const double cc = sqrt(kGamma * W.c[3] / W.c[0]);
+  const double s0 = 0.5 * (g.Si[(size_t)j * ni + i] + g.Si[(size_t)j * ni + ip]);
+  const double s1 = 0.5 * (g.Si[N + (size_t)j * ni + i] + g.Si[N + (size_t)j * ni + ip]);
+  const double t0 = 0.5 * (g.Sj[(size_t)(j + 1) * ni + i] + g.Sj[(size_t)j * ni + i]);
+  const double t1 = 0.5 * (g.Sj[NJ + (size_t)(j + 1) * ni + i] + g.Sj[NJ + (size_t)j * ni + i]);
+  const double li = fabs(W.c[1] * s0 + W.c[2] * s1) + cc * sqrt(s0 * s0 + s1 * s1);
+  const double lj = fabs(W.c[1] * t0 + W.c[2] * t1) + cc * sqrt(t0 * t0 + t1 * t1);
+  return cfl * g.vol[(size_t)j * ni + i] / (li + lj);
+}
+
+// local time steps of every case from its conserved state (the RK iteration)
 __global__ void __launch_bounds__(256) k_local_dt(Batch b, const double* __restrict__ U, double* __restrict__ dt,
                                                   double cfl) {
   const Tile t = b.tiles[blockIdx.x];
   const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
-  const int ni = g.ni, nc = g.nc;
-  const size_t N = (size_t)ni * nc, NJ = (size_t)(nc + 1) * ni;
   const double* Uc = U + 4 * cs.cell_off;
   for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
     const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
-    const int ip = (i + 1 == ni) ? 0 : i + 1;
     State4<double> u;
 #pragma unroll
     for (int k = 0; k < 4; ++k) u.c[k] = Uc[vidx(g, k, j, i)];
-    const State4<double> W = cons_to_prim<double, double>(u);
-    const double cc = sqrt(kGamma * W.c[3] / W.c[0]);
-    const double s0 = 0.5 * (g.Si[(size_t)j * ni + i] + g.Si[(size_t)j * ni + ip]);
-    const double s1 = 0.5 * (g.Si[N + (size_t)j * ni + i] + g.Si[N + (size_t)j * ni + ip]);
-    const double t0 = 0.5 * (g.Sj[(size_t)(j + 1) * ni + i] + g.Sj[(size_t)j * ni + i]);
-    const double t1 = 0.5 * (g.Sj[NJ + (size_t)(j + 1) * ni + i] + g.Sj[NJ + (size_t)j * ni + i]);
-    const double li = fabs(W.c[1] * s0 + W.c[2] * s1) + cc * sqrt(s0 * s0 + s1 * s1);
-    const double lj = fabs(W.c[1] * t0 + W.c[2] * t1) + cc * sqrt(t0 * t0 + t1 * t1);
-    dt[cs.cell_off + (size_t)j * ni + i] = cfl * g.vol[(size_t)j * ni + i] / (li + lj);
+    dt[cs.cell_off + (size_t)j * g.ni + i] = local_dt_cell(g, cons_to_prim<double, double>(u), j, i, cfl);
+  }
+}
+
+// local time steps of one case from primitives given in the reference layout
+// W[4][ni][nc], written as dt[ni][nc] (EulerSolver.local_dt, euler.py:289-296)
+__global__ void __launch_bounds__(256) k_local_dt_prim(GridDev g, const double* __restrict__ W,
+                                                       double* __restrict__ dt, double cfl) {
+  const size_t N = (size_t)g.ni * g.nc;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N; q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q / g.nc), j = (int)(q % g.nc);
+    State4<double> w;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) w.c[k] = W[k * N + q];
+    dt[q] = local_dt_cell(g, w, j, i, cfl);
   }
 }
 
@@ -300,6 +323,11 @@ __global__ void __launch_bounds__(256) k_fas_prolong(Batch fb, Batch cb, double*
 
 void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, cudaStream_t s) {
   if (b.ntiles) k_local_dt<<<b.ntiles, 256, 0, s>>>(b, U, dt, cfl);
+}
+void launch_local_dt_prim(const GridDev& g, const double* W, double* dt, double cfl, cudaStream_t s) {
+  const size_t N = (size_t)g.ni * g.nc;
+  const int blocks = (int)std::min<size_t>((N + 255) / 256, 148 * 8);
+  if (N) k_local_dt_prim<<<blocks, 256, 0, s>>>(g, W, dt, cfl);
 }
 void launch_irs(const Batch& b, double* R, double* tmp, double e, int max_ni, int max_nc, cudaStream_t s) {
   if (e <= 0.0 || b.ncases == 0) return;

@@ -7,6 +7,8 @@
 namespace a2d {
 
 void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, cudaStream_t s);
+// one case's local time steps from primitives in the reference layout W[4][ni][nc] -> dt[ni][nc]
+void launch_local_dt_prim(const GridDev& g, const double* W, double* dt, double cfl, cudaStream_t s);
 // R (in) -> tmp (out, smoothed along i then j)
 void launch_irs(const Batch& b, double* R, double* tmp, double e, int max_ni, int max_nc, cudaStream_t s);
 void launch_rk_stage(const Batch& b, const double* U0, const double* R, const double* dt, double* U, double a,

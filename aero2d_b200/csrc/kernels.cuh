@@ -26,6 +26,13 @@ template <> __device__ __forceinline__ __half from_f64<__half>(double v) {
   return __float2half_rn(fminf(fmaxf(f, -65504.0f), 65504.0f));
 }
 
+// 1 when a factor entry lies outside the storage type's finite range, i.e. the
+// FP16 store above saturates it (or it is not finite); never for FP32/FP64 storage
+template <typename TF> __device__ __forceinline__ unsigned out_of_range(double) { return 0u; }
+template <> __device__ __forceinline__ unsigned out_of_range<__half>(double v) {
+  return (fabs(v) <= 65504.0) ? 0u : 1u;
+}
+
 template <typename VT>
 struct StencilArgs {
   const double* U = nullptr;       // conserved state (FP64), packed cell vectors
@@ -68,6 +75,7 @@ struct FactorArgs {
                                    // Q = inv_j JIR(i+1) (to line i+1), G = -inv_j A_j  [rows nc]
   double* diag = nullptr;          // per-cell vol / dtau
   double cfl_base = 2.5;           // EulerSolver.cfl, which local_dt multiplies and step() divides out
+  unsigned long long* sat = nullptr; // counts factor entries saturated by the FP16 store
   uint32_t need = 0;
 };
 

@@ -201,7 +201,7 @@ __device__ __forceinline__ void load_block(const TJ* base, long long row0, int r
 // block m of the interleaved P, Q, G rows = A B (4x4, FP64), stored in TF (fbidx3)
 template <typename TF>
 __device__ __forceinline__ void mul4_store(const double A[16], const double B[16], TF* out, long long row0,
-                                           int rows, int g, int j, int m, int lane) {
+                                           int rows, int g, int j, int m, int lane, unsigned& nsat) {
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -209,6 +209,7 @@ __device__ __forceinline__ void mul4_store(const double A[16], const double B[16
       double s = A[r * 4 + 0] * B[0 * 4 + c];
 #pragma unroll
       for (int k = 1; k < 4; ++k) s += A[r * 4 + k] * B[k * 4 + c];
+      nsat += out_of_range<TF>(s);
       out[fbidx3(row0, rows, g, j, m, r, c, lane)] = from_f64<TF>(s);
     }
 }
@@ -237,6 +238,7 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   const double* U = a.U + 4 * cs.cell_off;
   const double cfl = a.ctl[grp.cs].cfl;
   const int k = nc / 2;   // twist row: the elimination from the wall and the one from the far field meet here
+  unsigned nsat = 0;      // factor entries this line stores saturated (FP16 storage)
   // D_j: the diagonal block of row j (face blocks + vol/dtau I); writes diag
   auto assemble = [&](int j, double D[16]) {
     double T1[16];
@@ -312,14 +314,15 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
     for (int e = 0; e < 16; ++e) {
       const size_t q = fbidx(cs.rows_nc, nc, grp.g, j, e >> 2, e & 3, lane);
       INV[q] = TJ(inv[e]);
+      nsat += out_of_range<TF>(Cm[e]) + out_of_range<TF>(Gm[e]);
       CF[q] = from_f64<TF>(Cm[e]);
       PQG[fbidx3(cs.rows_nc, nc, grp.g, j, 2, e >> 2, e & 3, lane)] = from_f64<TF>(Gm[e]);
     }
     double T1[16];
     load_block(JIL, cs.rows_nc, nc, grp.g, j, lane, T1);
-    mul4_store(inv, T1, PQG, cs.rows_nc, nc, grp.g, j, 0, lane);
+    mul4_store(inv, T1, PQG, cs.rows_nc, nc, grp.g, j, 0, lane, nsat);
     load_block(JIR, cs.rows_nc, nc, gp, j, lp, T1);
-    mul4_store(inv, T1, PQG, cs.rows_nc, nc, grp.g, j, 1, lane);
+    mul4_store(inv, T1, PQG, cs.rows_nc, nc, grp.g, j, 1, lane, nsat);
   };
   // The line system is L_j x_{j-1} + D_j x_j + U_j x_{j+1} = r_j with L_j = -JJL(j),
   // U_j = JJR(j+1) (aero2d/implicit.py:81-128).
@@ -371,6 +374,7 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
     mul(inv, Um, Hm, -1.0);
     store_row(k, inv, Gm, Hm);
   }
+  if (nsat != 0 && a.sat != nullptr) atomicAdd(a.sat, (unsigned long long)nsat);
 }
 
 template <typename T>

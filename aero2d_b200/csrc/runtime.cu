@@ -88,6 +88,7 @@ struct a2d_plan {
   size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_PQG = 0, o_V = 0;
   size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
   size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0, o_idx = 0;
+  size_t o_sat = 0;        // saturated FP16 factor entries since bind (a2d_factor_saturations)
   int pstride = 0;
   size_t bytes = 0;
   char* ws = nullptr;
@@ -191,6 +192,7 @@ static void layout(a2d_plan* P) {
   P->o_hcl = cv.take(8 * (size_t)B * P->p.max_iter);
   P->o_cnt = cv.take(8);   // [0] live-case count, [1] sweep copy-wait failure flag
   P->o_idx = cv.take(sizeof(int) * (size_t)B);   // case index lists of a2d_case_restart / _retire
+  P->o_sat = cv.take(sizeof(unsigned long long));
   P->bytes = cv.off + 256;
 }
 
@@ -294,6 +296,20 @@ __global__ void k_to_reference(int ni, int nc, const double* __restrict__ src, d
   }
 }
 
+// primitives of one case's cell vector, internal [4][nc][ni] -> reference [4][ni][nc]
+__global__ void k_to_reference_prim(int ni, int nc, const double* __restrict__ src, double* __restrict__ dst) {
+  const size_t N = (size_t)ni * nc;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N; q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q / nc), j = (int)(q % nc);
+    State4<double> u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) u.c[k] = src[((size_t)k * nc + j) * ni + i];
+    const State4<double> w = cons_to_prim<double, double>(u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dst[k * N + q] = w.c[k];
+  }
+}
+
 __global__ void k_point_flux(int n, const double* WL, const double* WR, const double* S, double* F) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
@@ -348,6 +364,7 @@ static FactorArgs factor_args(const a2d_plan* P, uint32_t need) {
   fa.PQG = P->at<void>(P->o_PQG);
   fa.diag = P->at<double>(P->o_diag);
   fa.cfl_base = P->p.cfl;
+  fa.sat = P->at<unsigned long long>(P->o_sat);
   fa.need = need;
   return fa;
 }
@@ -715,6 +732,7 @@ int a2d_plan_bind(a2d_plan* P, void* workspace, size_t bytes, void* stream) {
   B.ngroups = (int)P->groups.size();
   if (P->host_count == nullptr) A2D_CK(cudaMallocHost(&P->host_count, 2 * sizeof(int)));
   A2D_CK(cudaMemsetAsync(P->ws + P->o_cnt, 0, 8, s));
+  A2D_CK(cudaMemsetAsync(P->ws + P->o_sat, 0, sizeof(unsigned long long), s));
   A2D_CK(sweep_init());
   A2D_CK(gs_init());
   k_reset<<<(P->ncases + 63) / 64, 64, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.cfl0);
@@ -755,6 +773,26 @@ int a2d_vec_get(const a2d_plan* P, int slot, int k, double* dst, void* stream) {
   const CaseDev& c = P->cases[k];
   k_to_reference<<<256, 256, 0, static_cast<cudaStream_t>(stream)>>>(c.g.ni, c.g.nc,
                                                                       P->vec(slot) + 4 * c.cell_off, dst);
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_vec_get_prim(const a2d_plan* P, int slot, int k, double* dst, void* stream) {
+  A2D_BOUND(P);
+  if (int e = check_case(P, slot, k)) return e;
+  if (dst == nullptr) return fail(A2D_ERR_ARG, "null destination");
+  const CaseDev& c = P->cases[k];
+  k_to_reference_prim<<<256, 256, 0, static_cast<cudaStream_t>(stream)>>>(c.g.ni, c.g.nc,
+                                                                           P->vec(slot) + 4 * c.cell_off, dst);
+  A2D_CK(cudaGetLastError());
+  return A2D_OK;
+}
+
+int a2d_local_dt(const a2d_plan* P, int k, const double* W, double* dt, void* stream) {
+  A2D_BOUND(P);
+  if (k < 0 || k >= P->ncases) return fail(A2D_ERR_ARG, "local_dt: case index out of range");
+  if (W == nullptr || dt == nullptr) return fail(A2D_ERR_ARG, "local_dt: null pointer");
+  launch_local_dt_prim(P->cases[k].g, W, dt, P->p.cfl, static_cast<cudaStream_t>(stream));
   A2D_CK(cudaGetLastError());
   return A2D_OK;
 }
@@ -954,6 +992,16 @@ int a2d_newton_run(a2d_plan* P, int max_steps, int* steps, void* stream) {
     if (*P->host_count == 0) break;
   }
   if (steps != nullptr) *steps = done;
+  return A2D_OK;
+}
+
+int a2d_factor_saturations(a2d_plan* P, unsigned long long* count, int reset, void* stream) {
+  A2D_BOUND(P);
+  if (count == nullptr) return fail(A2D_ERR_ARG, "null output");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  A2D_CK(cudaMemcpyAsync(count, P->ws + P->o_sat, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  if (reset) A2D_CK(cudaMemsetAsync(P->ws + P->o_sat, 0, sizeof(unsigned long long), s));
+  A2D_CK(cudaStreamSynchronize(s));
   return A2D_OK;
 }
 

@@ -12,6 +12,7 @@
 // Every call rebuilds the tables and overwrites every partial it reads, so
 // nothing carries over between calls; calls whose kernels overlap on the GPU
 // (on two streams at once) share the array and race.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -77,21 +78,57 @@ __global__ void k_static_norms(const unsigned char* scratch, int ncases, int cel
   rnorm[k] = sqrt(s / (double)cells);
 }
 
-// device address of g_scratch, looked up once per device with that device current
+// device address of g_scratch for the calling thread's current context.  The
+// address is looked up (cudaGetSymbolAddress, with the device current) on the
+// first call on a device and again whenever that device's current context has
+// changed since (e.g. the primary context was destroyed by cudaDeviceReset and
+// re-created), since a module's symbols get new addresses in a new context.
+// The context is identified by cuCtxGetId, fetched through the runtime's driver
+// entry-point query, so the library needs no link against libcuda.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+
+static int current_context_id(unsigned long long* id) {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault) == cudaSuccess)
+      get_current = reinterpret_cast<PfnCtxGetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault) == cudaSuccess)
+      get_id = reinterpret_cast<PfnCtxGetId>(f);
+  });
+  *id = 0;
+  if (get_current == nullptr || get_id == nullptr)
+    return fail(A2D_ERR_CUDA, "residual_norms_static: the driver does not export cuCtxGetCurrent/cuCtxGetId");
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS) return fail(A2D_ERR_CUDA, "residual_norms_static: cuCtxGetCurrent failed");
+  if (ctx == nullptr) return A2D_OK;   // no context yet: id 0, the lookup creates the primary context
+  if (get_id(ctx, id) != CUDA_SUCCESS) return fail(A2D_ERR_CUDA, "residual_norms_static: cuCtxGetId failed");
+  return A2D_OK;
+}
+
 static int scratch_address(unsigned char** out) {
   static std::mutex mu;
   static unsigned char* addr[128] = {};
+  static unsigned long long ctx_of[128] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(A2D_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= 128) return fail(A2D_ERR_ARG, "device ordinal out of range");
+  unsigned long long ctx = 0;
+  if (int rc = current_context_id(&ctx)) return rc;
   std::lock_guard<std::mutex> lock(mu);
-  if (addr[dev] == nullptr) {
+  if (addr[dev] == nullptr || ctx == 0 || ctx != ctx_of[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess)
       return fail(A2D_ERR_CUDA, std::string("cudaGetSymbolAddress(g_scratch): ") + cudaGetErrorString(e));
+    if (ctx == 0 && current_context_id(&ctx) != A2D_OK) return A2D_ERR_CUDA;
     addr[dev] = static_cast<unsigned char*>(p);
+    ctx_of[dev] = ctx;
   }
   *out = addr[dev];
   return A2D_OK;

@@ -206,9 +206,13 @@ class EulerSolver:
         if circ is not None:
             c = torch.full((1,), float(circ), dtype=torch.float64, device=self.device)
         pl.residual(c)
-        R = pl.get_vec(_lib.VEC_R, 0)
-        Ut = torch.as_tensor(U, dtype=torch.float64, device=self.device)
-        return R, cons_to_prim(Ut)
+        return pl.get_vec(_lib.VEC_R, 0), pl.get_prim(_lib.VEC_U, 0)
+
+    def local_dt(self, W):
+        """Local time steps (ni, nc) of one case from its primitives W (4, ni, nc):
+        cfl * vol / (lambda_i + lambda_j) (aero2d/euler.py:289-296)."""
+        pl = self._plan(np.array([1.0, 0.5, 0.0, 1 / GAMMA]))
+        return pl.local_dt(0, W)
 
     def forces(self, U, winf):
         """(cl, cd, cm, cp) of one case (aero2d/euler.py:318-331)."""

@@ -125,6 +125,25 @@ class Plan:
             _lib.check(self.lib.a2d_vec_get(self.handle, slot, k, _ptr(out), self.stream))
         return out
 
+    def get_prim(self, slot: int, k: int) -> torch.Tensor:
+        """Primitives (rho, u, v, p) of a slot's vector of case k, (4, ni, nc)."""
+        g = self.grids[k]
+        out = torch.empty((4, g.ni, g.nc), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.a2d_vec_get_prim(self.handle, slot, k, _ptr(out), self.stream))
+        return out
+
+    def local_dt(self, k: int, W) -> torch.Tensor:
+        """Local time steps (ni, nc) of case k from primitives W (4, ni, nc)."""
+        g = self.grids[k]
+        W = torch.as_tensor(W, dtype=torch.float64, device=self.device).contiguous()
+        if tuple(W.shape) != (4, g.ni, g.nc):
+            raise ValueError(f"W of case {k} must have shape (4, {g.ni}, {g.nc}), got {tuple(W.shape)}")
+        dt = torch.empty((g.ni, g.nc), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.a2d_local_dt(self.handle, k, _ptr(W), _ptr(dt), self.stream))
+        return dt
+
     def set_batch(self, slot: int, U: torch.Tensor) -> None:
         for k in range(self.B):
             self.set_vec(slot, k, U[k])
@@ -186,6 +205,12 @@ class Plan:
         n = C.c_int()
         self.call("a2d_live_count", C.byref(n))
         return n.value
+
+    def factor_saturations(self, reset: bool = False) -> int:
+        """Sweep-factor entries stored saturated in FP16 since bind (mixed plans)."""
+        n = C.c_ulonglong()
+        self.call("a2d_factor_saturations", C.byref(n), int(bool(reset)))
+        return int(n.value)
 
     def stats(self):
         """(kernel launches per Newton step, Newton steps since reset)."""

@@ -102,6 +102,9 @@ int a2d_plan_ncases(const a2d_plan* plan);
 /* vector I/O in the reference layout [4][ni][nc] of one case (device pointers) */
 int a2d_vec_set(a2d_plan* plan, int slot, int case_index, const double* src, void* stream);
 int a2d_vec_get(const a2d_plan* plan, int slot, int case_index, double* dst, void* stream);
+/* primitives (rho, u, v, p) = cons_to_prim of a slot's vector of one case (euler.py:66-71),
+ * in the reference layout [4][ni][nc]: the W that EulerSolver.residual returns (euler.py:260) */
+int a2d_vec_get_prim(const a2d_plan* plan, int slot, int case_index, double* dst, void* stream);
 
 /* ---- point operations (aero2d/euler.py) ---- */
 /* U of every case := prim_to_cons(winf) (init_state, euler.py:383-384); resets the Newton state */
@@ -120,6 +123,9 @@ int a2d_forces(a2d_plan* plan, double* coef, double* cp, void* stream);
 int a2d_precond_setup(a2d_plan* plan, void* stream);
 /* JV := M(V), the line-Jacobi application (implicit.py:150-157) */
 int a2d_precond_apply(a2d_plan* plan, void* stream);
+/* local time steps of case case_index from primitives W (device [4][ni][nc], reference layout):
+ * dt [ni][nc] = params.cfl * vol / (lambda_i + lambda_j) (EulerSolver.local_dt, euler.py:289-296) */
+int a2d_local_dt(const a2d_plan* plan, int case_index, const double* W, double* dt, void* stream);
 /* sets the pseudo-time CFL of every case (host array [ncases]) */
 int a2d_set_cfl(a2d_plan* plan, const double* cfl, void* stream);
 
@@ -195,6 +201,11 @@ int a2d_service_destroy(a2d_service* service);
 /* per-step histories to host arrays [steps][ncases] (residual norm, Cl); steps <= max_iter */
 int a2d_history(const a2d_plan* plan, int steps, double* rn, double* cl, void* stream);
 
+/* sweep-factor entries (G, C, P, Q) that the mixed-precision factorisation stored saturated
+ * since bind (or the last reset): entries beyond the FP16 range (|v| > 65504, or not finite) are
+ * stored as +-65504; FP64 plans never saturate.  *count to host; reset != 0 zeroes the counter;
+ * synchronises.  No counterpart in the reference (it factors in the solver dtype) */
+int a2d_factor_saturations(a2d_plan* plan, unsigned long long* count, int reset, void* stream);
 /* number of cases still stepping (retire=1) or not yet done (retire=0); synchronises */
 int a2d_live_count(a2d_plan* plan, int* n, void* stream);
 /* kernel launches of one Newton step (counted in the captured graph; 0 before the
@@ -241,8 +252,9 @@ int a2d_set_circulation(a2d_plan* plan, const double* circ, void* stream);
  * residual norm rnorm[k] = sqrt(mean((R_rho / vol)^2)) that the Newton loop tests for
  * convergence.  It allocates nothing: besides the caller's buffers it uses one file-scope
  * device array of about 0.86 MB, which every GPU that loads the library holds until the process
- * exits; the first call on a device looks up that array's address, so make the first call on
- * each device before any stream capture.  Calls share the array, so calls whose kernels overlap
+ * exits; the first call on a device looks up that array's address (and a call looks it up again
+ * when the device's current context has changed since, e.g. after cudaDeviceReset), so make the
+ * first call on each device, and the first after such a change, before any stream capture.  Calls share the array, so calls whose kernels overlap
  * on the GPU race.  Limits: ncases <= 64, 4 <= ni <= 512, 2 <= nj - 1 <= 128; larger batches are
  * rejected with A2D_ERR_ARG.
  *   metrics: the grid's blob from a2d_metrics_build; U, R: device [ncases][4][nj-1][ni]

@@ -30,6 +30,26 @@ def perturbed_state(model: EulerModel, winf, seed=0, amp=0.02):
     return prim_to_cons(W)
 
 
+def transonic_draw(n=8, seed=2025):
+    """The transonic cases: random NACA 4-digit sections (m ~ U[0, 0.06],
+    p ~ U[0.2, 0.6], t ~ U[0.08, 0.16], 193 points per side), each on its own
+    384 x 96 O-grid (ds0 1e-3, radius 20; sections whose grid folds are redrawn),
+    then M ~ U[0.70, 0.80] and alpha ~ U[0, 3] deg, from default_rng(seed).
+    Returns (params [(m, p, t)], grids, machs, alphas, redrawn)."""
+    from aero2d_b200.grid import GridError
+    rng = np.random.default_rng(seed)
+    params, grids, rejected = [], [], 0
+    while len(grids) < n:
+        m, p, t = rng.uniform(0, 0.06), rng.uniform(0.2, 0.6), rng.uniform(0.08, 0.16)
+        try:
+            grids.append(ogrid(naca4_params(m, p, t, 193), nj=97, ds0=1e-3, radius=20.0))
+            params.append((float(m), float(p), float(t)))
+        except GridError:
+            rejected += 1
+    machs, alphas = rng.uniform(0.70, 0.80, n), rng.uniform(0.0, 3.0, n)
+    return params, grids, machs, alphas, rejected
+
+
 def decode_metrics(blob: np.ndarray, ni: int, nc: int):
     """Split the device metrics blob (uint8) into its FP64 arrays in the
     reference layout: vol (ni, nc), Si (2, ni, nc), Sj (2, ni, nc+1), xf, yf, xw, yw."""
@@ -44,4 +64,4 @@ def decode_metrics(blob: np.ndarray, ni: int, nc: int):
     return vol, Si, Sj, xf, yf, xw, yw
 
 
-__all__ = ["grid", "perturbed_state", "decode_metrics", "naca4", "naca4_params", "ogrid"]
+__all__ = ["grid", "perturbed_state", "transonic_draw", "decode_metrics", "naca4", "naca4_params", "ogrid"]

@@ -43,7 +43,7 @@ def test_transonic_mixed_vs_fp64(cuda):
         out[dt] = (~frozen & (lastrn < 1e-8 * r0), coef.cpu().numpy(), [c.cpu().numpy() for c in cps])
         pl.close()
     ok = out[np.float64][0] & out[np.float32][0]
-    assert ok.sum() >= 1, f"only {ok.sum()} of {B} transonic cases fell 8 orders in both precisions"
+    assert ok.sum() >= 3, f"only {ok.sum()} of {B} transonic cases fell 8 orders in both precisions"
     shocks = 0
     for k in np.nonzero(ok)[0]:
         c64, c32 = out[np.float64][1][k], out[np.float32][1][k]
