@@ -20,6 +20,10 @@ A2D_ERR_STATE = 3
 A2D_FP64 = 0
 A2D_MIXED = 1
 
+# tuning knobs (a2d_plan_set_tuning)
+JVP_TILES = {"32x8": 0, "32x16": 1, "64x4": 2, "16x16": 3}
+SWEEP_VARIANTS = {"lanes": 0, "rows": 1}
+
 VEC_U, VEC_R, VEC_V, VEC_JV, VEC_DU = 0, 1, 2, 3, 4
 
 # kernels that a2d_time_kernel can time
@@ -78,6 +82,8 @@ SIGNATURES = {
     "a2d_plan_bind": (_I, [_P, _P, _SZ, _P]),
     "a2d_plan_destroy": (_I, [_P]),
     "a2d_plan_ncases": (_I, [_P]),
+    "a2d_plan_set_tuning": (_I, [_P, _I, _I, _P]),
+    "a2d_plan_get_tuning": (_I, [_P, C.POINTER(_I), C.POINTER(_I)]),
     "a2d_vec_set": (_I, [_P, _I, _I, _P, _P]),
     "a2d_vec_get": (_I, [_P, _I, _I, _P, _P]),
     "a2d_vec_get_prim": (_I, [_P, _I, _I, _P, _P]),
@@ -116,7 +122,10 @@ SIGNATURES = {
     "a2d_service_poll": (_I, [_P, C.POINTER(C.c_longlong), _I, C.POINTER(_I)]),
     "a2d_service_result": (_I, [_P, C.c_longlong, C.POINTER(_D), C.POINTER(_D), C.POINTER(_I), C.POINTER(_I)]),
     "a2d_service_pending": (_I, [_P, C.POINTER(_I), C.POINTER(_I)]),
+    "a2d_service_result_drop": (_I, [_P, C.c_longlong, C.POINTER(_D)]),
     "a2d_service_destroy": (_I, [_P]),
+    "a2d_service_stats": (_I, [_P, C.POINTER(_I), C.POINTER(C.c_longlong)]),
+    "a2d_service_plan": (_I, [_P, C.POINTER(_P)]),
     "a2d_plan_set_coarse": (_I, [_P, _P]),
     "a2d_case_set_grid": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_P), _P]),
     "a2d_service_create_ragged": (_I, [_I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_P), C.POINTER(_I),

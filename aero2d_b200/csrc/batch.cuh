@@ -20,6 +20,16 @@ namespace a2d {
 
 constexpr int kTI = 32;        // stencil tile width  (i, circumferential cells)
 constexpr int kTJ = 8;         // stencil tile height (j, wall-normal cells)
+
+// tile shapes of the FP32 linearised stencil (the JVP), a plan's tuning knob;
+// every other tile kernel uses kTI x kTJ
+enum : int { kTile32x8 = 0, kTile32x16 = 1, kTile64x4 = 2, kTile16x16 = 3, kNumTileShapes = 4 };
+__host__ __device__ constexpr int tile_w(int shape) {
+  return shape == kTile64x4 ? 64 : (shape == kTile16x16 ? 16 : 32);
+}
+__host__ __device__ constexpr int tile_h(int shape) {
+  return shape == kTile32x16 || shape == kTile16x16 ? 16 : (shape == kTile64x4 ? 4 : 8);
+}
 constexpr int kLanes = 32;     // j-lines per line group
 constexpr int kChunk = 4096;   // vector entries per reduction chunk (16 per thread of a 256-thread CTA)
 constexpr int kMaxRestart = 64;

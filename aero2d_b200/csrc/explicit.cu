@@ -18,23 +18,24 @@ namespace a2d {
 
 // local time step of cell (j, i) from its primitives W = (rho, u, v, p):
 // dt = cfl vol / (lambda_i + lambda_j), face vectors averaged to the cell
-// centre, in the operation order of euler.py:289-296
-__device__ __forceinline__ double local_dt_cell(const GridDev& g, const State4<double>& W, int j, int i,
-                                                double cfl) {
-  const int ni = g.ni, nc = g.nc;
-  const size_t N = (size_t)ni * nc, NJ = (size_t)(nc + 1) * ni;
-  const int ip = (i + 1 == ni) ? 0 : i + 1;
-  const double cc = sqrt(kGamma * W.c[3] / W.c[0]);
-  const double s0 = 0.5 * (g.Si[(size_t)j * ni + i] + g.Si[(size_t)j * ni + ip]);
-  const double s1 = 0.5 * (g.Si[N + (size_t)j * ni + i] + g.Si[N + (size_t)j * ni + ip]);
-  const double t0 = 0.5 * (g.Sj[(size_t)(j + 1) * ni + i] + g.Sj[(size_t)j * ni + i]);
-  const double t1 = 0.5 * (g.Sj[NJ + (size_t)(j + 1) * ni + i] + g.Sj[NJ + (size_t)j * ni + i]);
-  const double li = fabs(W.c[1] * s0 + W.c[2] * s1) + cc * sqrt(s0 * s0 + s1 * s1);
-  const double lj = fabs(W.c[1] * t0 + W.c[2] * t1) + cc * sqrt(t0 * t0 + t1 * t1);
-  return cfl * g.vol[(size_t)j * ni + i] / (li + lj);
+// centre, in the operation order of euler.py:289-296; T is the compute type
+// (FP32 reads the grid's FP32 metric copies)
+template <typename T>
+__device__ __forceinline__ T local_dt_cell(const GridDev& g, const State4<T>& W, int j, int i, T cfl) {
+  const Metric<T> m{g};
+  const int ip = (i + 1 == g.ni) ? 0 : i + 1;
+  const T cc = sqrt(T(kGamma) * W.c[3] / W.c[0]);
+  const T s0 = T(0.5) * (m.si(0, j, i) + m.si(0, j, ip));
+  const T s1 = T(0.5) * (m.si(1, j, i) + m.si(1, j, ip));
+  const T t0 = T(0.5) * (m.sj(0, j + 1, i) + m.sj(0, j, i));
+  const T t1 = T(0.5) * (m.sj(1, j + 1, i) + m.sj(1, j, i));
+  const T li = fabs(W.c[1] * s0 + W.c[2] * s1) + cc * sqrt(s0 * s0 + s1 * s1);
+  const T lj = fabs(W.c[1] * t0 + W.c[2] * t1) + cc * sqrt(t0 * t0 + t1 * t1);
+  return cfl * m.vol(j, i) / (li + lj);
 }
 
 // local time steps of every case from its conserved state (the RK iteration)
+template <typename T>
 __global__ void __launch_bounds__(256) k_local_dt(Batch b, const double* __restrict__ U, double* __restrict__ dt,
                                                   double cfl) {
   const Tile t = b.tiles[blockIdx.x];
@@ -43,10 +44,10 @@ __global__ void __launch_bounds__(256) k_local_dt(Batch b, const double* __restr
   const double* Uc = U + 4 * cs.cell_off;
   for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
     const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
-    State4<double> u;
+    State4<T> u;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) u.c[k] = Uc[vidx(g, k, j, i)];
-    dt[cs.cell_off + (size_t)j * g.ni + i] = local_dt_cell(g, cons_to_prim<double, double>(u), j, i, cfl);
+    for (int k = 0; k < 4; ++k) u.c[k] = T(Uc[vidx(g, k, j, i)]);
+    dt[cs.cell_off + (size_t)j * g.ni + i] = (double)local_dt_cell<T>(g, cons_to_prim<T, T>(u), j, i, T(cfl));
   }
 }
 
@@ -60,13 +61,15 @@ __global__ void __launch_bounds__(256) k_local_dt_prim(GridDev g, const double* 
     State4<double> w;
 #pragma unroll
     for (int k = 0; k < 4; ++k) w.c[k] = W[k * N + q];
-    dt[q] = local_dt_cell(g, w, j, i, cfl);
+    dt[q] = local_dt_cell<double>(g, w, j, i, cfl);
   }
 }
 
-// periodic smoothing along i: one block per (case, component, row j)
+// periodic smoothing along i: one block per (case, component, row j); T is the
+// compute type (values stay in FP64 arrays, rounded to T when T is FP32)
+template <typename T>
 __global__ void __launch_bounds__(256) k_irs_i(Batch b, const double* __restrict__ R, double* __restrict__ out,
-                                               double e) {
+                                               double e_) {
   const int row = blockIdx.x;   // rows enumerated as (case, k, j) via the row table below
   const int cs_id = blockIdx.y;
   const CaseDev cs = b.cases[cs_id];
@@ -74,23 +77,26 @@ __global__ void __launch_bounds__(256) k_irs_i(Batch b, const double* __restrict
   const int ni = g.ni, nc = g.nc;
   if (row >= 4 * nc) return;
   const int k = row / nc, j = row % nc;
-  extern __shared__ double sm[];
-  double* r = sm;          // ni
-  double* gm = sm + ni;    // up to ni/2 + 1
+  extern __shared__ __align__(8) unsigned char irs_sm[];
+  T* r = reinterpret_cast<T*>(irs_sm);   // ni
+  T* gm = r + ni;                         // up to ni/2 + 1
   const double* src = R + 4 * cs.cell_off + vidx(g, k, j, 0);
-  for (int i = threadIdx.x; i < ni; i += blockDim.x) r[i] = src[i];
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) r[i] = T(src[i]);
+  // the Green's function in FP64, then rounded to T (its terms below 1e-18 of
+  // the diagonal dropped: the FFT's solution to rounding)
+  const double e = e_;
   const double lam = ((1.0 + 2.0 * e) - sqrt(1.0 + 4.0 * e)) / (2.0 * e);
   const double G0 = 1.0 / (e * (1.0 / lam - lam));
   int M = (int)ceil(log(1e-18) / log(lam));
   if (M > ni / 2) M = ni / 2;
   const double ln = pow(lam, (double)ni);
   for (int m = threadIdx.x; m <= M; m += blockDim.x)
-    gm[m] = G0 * (pow(lam, (double)m) + pow(lam, (double)(ni - m))) / (1.0 - ln);
+    gm[m] = T(G0 * (pow(lam, (double)m) + pow(lam, (double)(ni - m))) / (1.0 - ln));
   __syncthreads();
   double* dst = out + 4 * cs.cell_off + vidx(g, k, j, 0);
   const bool full = (2 * M + 1 >= ni);
   for (int i = threadIdx.x; i < ni; i += blockDim.x) {
-    double s = gm[0] * r[i];
+    T s = gm[0] * r[i];
     if (full) {
       for (int d = 1; d < ni; ++d) {
         const int m = d <= ni / 2 ? d : ni - d;
@@ -106,24 +112,27 @@ __global__ void __launch_bounds__(256) k_irs_i(Batch b, const double* __restrict
         s += gm[m] * (r[qm] + r[qp]);
       }
     }
-    dst[i] = s;
+    dst[i] = (double)s;
   }
 }
 
 // smoothing along j: Thomas solve per (case, component, line i); thread per line.
 // The elimination coefficients depend on j only and are formed once per block.
-__global__ void __launch_bounds__(128) k_irs_j(Batch b, double* __restrict__ R, double e) {
+template <typename T>
+__global__ void __launch_bounds__(128) k_irs_j(Batch b, double* __restrict__ R, double e_) {
   const int cs_id = blockIdx.y;
   const CaseDev cs = b.cases[cs_id];
   const GridDev& g = cs.g;
   const int ni = g.ni, nc = g.nc;
-  extern __shared__ double cpj[];   // nc
+  extern __shared__ __align__(8) unsigned char irs_sm[];
+  T* cpj = reinterpret_cast<T*>(irs_sm);   // nc
+  const T e = T(e_);
   if (threadIdx.x == 0) {
-    double cp = 0.0;
+    T cp = T(0);
     for (int j = 0; j < nc; ++j) {
-      const double dj = (j == 0 || j == nc - 1) ? 1.0 + e : 1.0 + 2.0 * e;
-      const double lj = (j == 0) ? 0.0 : -e;
-      const double uj = (j == nc - 1) ? 0.0 : -e;
+      const T dj = (j == 0 || j == nc - 1) ? T(1) + e : T(1) + T(2) * e;
+      const T lj = (j == 0) ? T(0) : -e;
+      const T uj = (j == nc - 1) ? T(0) : -e;
       cp = uj / (dj - lj * cp);
       cpj[j] = cp;
     }
@@ -133,39 +142,42 @@ __global__ void __launch_bounds__(128) k_irs_j(Batch b, double* __restrict__ R, 
   if (line >= 4 * ni) return;
   const int k = line / ni, i = line % ni;
   double* x = R + 4 * cs.cell_off;
-  double dprev = 0.0;
+  T dprev = T(0);
   for (int j = 0; j < nc; ++j) {
-    const double dj = (j == 0 || j == nc - 1) ? 1.0 + e : 1.0 + 2.0 * e;
-    const double lj = (j == 0) ? 0.0 : -e;
-    const double den = dj - lj * (j == 0 ? 0.0 : cpj[j - 1]);
-    const double v = (x[vidx(g, k, j, i)] - lj * dprev) / den;
-    x[vidx(g, k, j, i)] = v;
+    const T dj = (j == 0 || j == nc - 1) ? T(1) + e : T(1) + T(2) * e;
+    const T lj = (j == 0) ? T(0) : -e;
+    const T den = dj - lj * (j == 0 ? T(0) : cpj[j - 1]);
+    const T v = (T(x[vidx(g, k, j, i)]) - lj * dprev) / den;
+    x[vidx(g, k, j, i)] = (double)v;
     dprev = v;
   }
-  double xn = 0.0;
+  T xn = T(0);
   for (int j = nc - 1; j >= 0; --j) {
-    const double v = x[vidx(g, k, j, i)] - cpj[j] * xn;
-    x[vidx(g, k, j, i)] = v;
+    const T v = T(x[vidx(g, k, j, i)]) - cpj[j] * xn;
+    x[vidx(g, k, j, i)] = (double)v;
     xn = v;
   }
 }
 
-// U = U0 - a (dt / vol) R   (euler.py:344)
+// U = U0 - a (dt / vol) R   (euler.py:344), in the compute type T (with FP32
+// the state is rounded to FP32 at every stage, as the reference's float32 run keeps it)
+template <typename T>
 __global__ void __launch_bounds__(256) k_rk_stage(Batch b, const double* __restrict__ U0,
                                                   const double* __restrict__ R, const double* __restrict__ dt,
                                                   double* __restrict__ U, double a) {
   const Tile t = b.tiles[blockIdx.x];
   const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
+  const Metric<T> m{g};
   const size_t base = 4 * cs.cell_off;
   for (int c = threadIdx.x; c < t.ti * t.tj; c += blockDim.x) {
     const int j = t.j0 + c / t.ti, i = t.i0 + c % t.ti;
     const size_t cell = (size_t)j * g.ni + i;
-    const double f = a * (dt[cs.cell_off + cell] / g.vol[cell]);
+    const T f = T(a) * (T(dt[cs.cell_off + cell]) / m.vol(j, i));
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const size_t q = base + vidx(g, k, j, i);
-      U[q] = U0[q] - f * R[q];
+      U[q] = (double)(T(U0[q]) - f * T(R[q]));
     }
   }
 }
@@ -321,25 +333,35 @@ __global__ void __launch_bounds__(256) k_fas_prolong(Batch fb, Batch cb, double*
   }
 }
 
-void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, cudaStream_t s) {
-  if (b.ntiles) k_local_dt<<<b.ntiles, 256, 0, s>>>(b, U, dt, cfl);
+void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, bool fp32, cudaStream_t s) {
+  if (b.ntiles == 0) return;
+  if (fp32) k_local_dt<float><<<b.ntiles, 256, 0, s>>>(b, U, dt, cfl);
+  else k_local_dt<double><<<b.ntiles, 256, 0, s>>>(b, U, dt, cfl);
 }
 void launch_local_dt_prim(const GridDev& g, const double* W, double* dt, double cfl, cudaStream_t s) {
   const size_t N = (size_t)g.ni * g.nc;
   const int blocks = (int)std::min<size_t>((N + 255) / 256, 148 * 8);
   if (N) k_local_dt_prim<<<blocks, 256, 0, s>>>(g, W, dt, cfl);
 }
-void launch_irs(const Batch& b, double* R, double* tmp, double e, int max_ni, int max_nc, cudaStream_t s) {
+void launch_irs(const Batch& b, double* R, double* tmp, double e, int max_ni, int max_nc, bool fp32,
+                cudaStream_t s) {
   if (e <= 0.0 || b.ncases == 0) return;
   dim3 gi(4 * max_nc, b.ncases);
   const size_t sm = (size_t)(max_ni + max_ni / 2 + 2) * sizeof(double);
-  k_irs_i<<<gi, 256, sm, s>>>(b, R, tmp, e);
   dim3 gj((4 * max_ni + 127) / 128, b.ncases);
-  k_irs_j<<<gj, 128, (size_t)max_nc * sizeof(double), s>>>(b, tmp, e);
+  if (fp32) {
+    k_irs_i<float><<<gi, 256, sm, s>>>(b, R, tmp, e);
+    k_irs_j<float><<<gj, 128, (size_t)max_nc * sizeof(double), s>>>(b, tmp, e);
+  } else {
+    k_irs_i<double><<<gi, 256, sm, s>>>(b, R, tmp, e);
+    k_irs_j<double><<<gj, 128, (size_t)max_nc * sizeof(double), s>>>(b, tmp, e);
+  }
 }
 void launch_rk_stage(const Batch& b, const double* U0, const double* R, const double* dt, double* U, double a,
-                     cudaStream_t s) {
-  if (b.ntiles) k_rk_stage<<<b.ntiles, 256, 0, s>>>(b, U0, R, dt, U, a);
+                     bool fp32, cudaStream_t s) {
+  if (b.ntiles == 0) return;
+  if (fp32) k_rk_stage<float><<<b.ntiles, 256, 0, s>>>(b, U0, R, dt, U, a);
+  else k_rk_stage<double><<<b.ntiles, 256, 0, s>>>(b, U0, R, dt, U, a);
 }
 void launch_rk_res(const Batch& b, const double* U0, const double* U, const double* dt, double* tpart,
                    cudaStream_t s) {

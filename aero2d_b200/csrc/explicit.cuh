@@ -6,13 +6,15 @@
 
 namespace a2d {
 
-void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, cudaStream_t s);
+// fp32: the explicit iteration's FP32 form (compute in FP32, values kept in the FP64 arrays)
+void launch_local_dt(const Batch& b, const double* U, double* dt, double cfl, bool fp32, cudaStream_t s);
 // one case's local time steps from primitives in the reference layout W[4][ni][nc] -> dt[ni][nc]
 void launch_local_dt_prim(const GridDev& g, const double* W, double* dt, double cfl, cudaStream_t s);
 // R (in) -> tmp (out, smoothed along i then j)
-void launch_irs(const Batch& b, double* R, double* tmp, double e, int max_ni, int max_nc, cudaStream_t s);
+void launch_irs(const Batch& b, double* R, double* tmp, double e, int max_ni, int max_nc, bool fp32,
+                cudaStream_t s);
 void launch_rk_stage(const Batch& b, const double* U0, const double* R, const double* dt, double* U, double a,
-                     cudaStream_t s);
+                     bool fp32, cudaStream_t s);
 void launch_rk_res(const Batch& b, const double* U0, const double* U, const double* dt, double* tpart,
                    cudaStream_t s);
 void launch_rk_finish(const Batch& b, const double* tpart, const double* coef, double* res, double* circ,

@@ -102,8 +102,13 @@ struct SweepArgs {
 void launch_metrics(int ni, int nc, const double* x, const double* y, double* md, float* mf,
                     cudaStream_t s);
 
+// shape: the tile shape of b's tile list (kTile*; only the FP32 linearised
+// stencil has shapes other than kTile32x8)
 template <typename T, bool LIN, typename VT>
-void launch_stencil(const Batch& b, const StencilArgs<VT>& a, cudaStream_t s);
+void launch_stencil(const Batch& b, const StencilArgs<VT>& a, cudaStream_t s, int shape = kTile32x8);
+// resident-CTA queries of the persistent stencil launches (host, before any capture)
+void stencil_init_fp64();
+void stencil_init_fp32();
 
 void launch_forces(const Batch& b, const double* U, double* coef, double* cp, const long long* cp_off,
                    const CaseCtl* ctl, double* hist_cl, int hist_cap, cudaStream_t s);
@@ -114,12 +119,21 @@ void launch_face_jac(const Batch& b, const JacArgs& a, cudaStream_t s);
 template <typename TJ, typename TF>
 void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s);
 
-// one line-Jacobi sweep (sweep.cu); FIRST: the sweep without i-coupling;
-// last: x is the FP64 result (else an intermediate vector)
+// kernel variants of the line-Jacobi sweep, a plan's tuning knob: one warp per
+// half line group, a lane solving all four block rows of its line (sweep.cu), or
+// four warps per half line group, a warp per block row (sweep_rows.cu)
+enum : int { kSweepLanes = 0, kSweepRows = 1, kNumSweepVariants = 2 };
+
+// one line-Jacobi sweep; FIRST: the sweep without i-coupling; last: x is the
+// FP64 result (else an intermediate vector).  Both variants compute the same
+// arithmetic in the same order
 template <typename TI, bool FIRST>
-void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s);
+void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s, int variant = kSweepLanes);
+template <typename TI, bool FIRST>
+void launch_sweep_rows(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s);
 
 // raises the dynamic shared-memory limit of the sweep kernels (host, once per device)
 cudaError_t sweep_init();
+cudaError_t sweep_rows_init();
 
 }  // namespace a2d

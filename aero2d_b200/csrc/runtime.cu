@@ -76,6 +76,10 @@ struct a2d_plan {
   int max_ni = 0, max_nc = 0;
   std::vector<CaseDev> cases;
   std::vector<Tile> tiles;
+  std::vector<Tile> jtiles;    // tiles of the FP32 linearised stencil, in the shape jvp_tile
+  int jvp_tile = kTile32x8;    // tuning knobs (a2d_plan_set_tuning)
+  int sweep_variant = kSweepLanes;
+  int max_jtiles = 0;          // the most tiles any JVP tile shape needs (workspace room)
   std::vector<Chunk> chunks;
   std::vector<Group> groups;
   std::vector<long long> cp_off;
@@ -89,6 +93,8 @@ struct a2d_plan {
   size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
   size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0, o_idx = 0;
   size_t o_sat = 0;        // saturated FP16 factor entries since bind (a2d_factor_saturations)
+  size_t o_jtiles = 0;
+  Batch jbatch{};          // the batch with the JVP's tile list
   int pstride = 0;
   size_t bytes = 0;
   char* ws = nullptr;
@@ -111,6 +117,19 @@ namespace a2d {
 // ---------------------------------------------------------------------------
 // plan construction
 // ---------------------------------------------------------------------------
+// tiles of every case in the given shape, case after case
+static std::vector<Tile> tile_list(const a2d_plan* P, int shape) {
+  const int TI = tile_w(shape), TJ = tile_h(shape);
+  std::vector<Tile> out;
+  for (int k = 0; k < P->ncases; ++k) {
+    const int ni = P->cases[k].g.ni, nc = P->cases[k].g.nc;
+    for (int j0 = 0; j0 < nc; j0 += TJ)
+      for (int i0 = 0; i0 < ni; i0 += TI)
+        out.push_back(Tile{k, i0, j0, std::min(TI, ni - i0), std::min(TJ, nc - j0)});
+  }
+  return out;
+}
+
 static void build_tables(a2d_plan* P, const int* ni, const int* nc, const void* const* metrics,
                          const double* winf) {
   long long cell = 0, rnc = 0, rnc1 = 0, cpo = 0;
@@ -149,6 +168,8 @@ static void build_tables(a2d_plan* P, const int* ni, const int* nc, const void* 
   P->rows_nc = rnc;
   P->rows_nc1 = rnc1;
   P->total_ni = cpo;
+  for (int sh = 0; sh < kNumTileShapes; ++sh) P->max_jtiles = std::max(P->max_jtiles, (int)tile_list(P, sh).size());
+  P->jtiles = tile_list(P, P->jvp_tile);
 }
 
 static void layout(a2d_plan* P) {
@@ -193,6 +214,7 @@ static void layout(a2d_plan* P) {
   P->o_cnt = cv.take(8);   // [0] live-case count, [1] sweep copy-wait failure flag
   P->o_idx = cv.take(sizeof(int) * (size_t)B);   // case index lists of a2d_case_restart / _retire
   P->o_sat = cv.take(sizeof(unsigned long long));
+  P->o_jtiles = cv.take(sizeof(Tile) * (size_t)P->max_jtiles);
   P->bytes = cv.off + 256;
 }
 
@@ -379,12 +401,12 @@ static void precond(a2d_plan* P, const Batch& B, const double* rin, double* dst,
   a.r = rin;
   a.e0 = sweeps > 1 ? P->vec(kPE) : nullptr;
   a.x = sweeps > 1 ? bufs[0] : dst;
-  launch_sweep<TJ, true>(B, a, sweeps == 1, s);
+  launch_sweep<TJ, true>(B, a, sweeps == 1, s, P->sweep_variant);
   for (int sw = 1; sw < sweeps; ++sw) {
     const bool last = sw == sweeps - 1;
     a.xprev = a.x;
     a.x = last ? dst : bufs[sw & 1];
-    launch_sweep<TJ, false>(B, a, last, s);
+    launch_sweep<TJ, false>(B, a, last, s, P->sweep_variant);
   }
 }
 
@@ -410,6 +432,19 @@ static StencilArgs<double> residual_args(a2d_plan* P) {
   a.order = P->p.order;
   a.vortex = P->p.vortex_correction;
   return a;
+}
+
+// the linearised stencil (J v): in FP32 on the plan's JVP tile list and shape,
+// in FP64 on the standard tiles
+template <typename TV, typename VT>
+static void launch_jvp(const a2d_plan* P, const StencilArgs<VT>& a, cudaStream_t s) {
+  if constexpr (sizeof(TV) == 4) {
+    Batch jb = P->jbatch;
+    jb.live = P->batch.live;
+    launch_stencil<TV, true, VT>(jb, a, s, P->jvp_tile);
+  } else {
+    launch_stencil<TV, true, VT>(P->batch, a, s);
+  }
 }
 
 template <typename TV, typename TJ, typename TB>
@@ -458,7 +493,7 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
   ta.bvec = b;
   ta.out = t;
   ta.need = NW;
-  launch_stencil<TV, true, double>(B, ta, s);
+  launch_jvp<TV, double>(P, ta, s);
   // r = M t, v0 = r / ||r||
   precond<TJ>(P, B, t, r, NW, s);
   double* h1 = P->at<double>(P->o_h1);
@@ -492,7 +527,7 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
     za.order = P->p.order;
     za.vortex = P->p.vortex_correction;
     za.need = KR;
-    launch_stencil<TV, true, TB>(B, za, s);
+    launch_jvp<TV, TB>(P, za, s);
     precond<TJ>(P, B, z, w, KR, s);
     // classical Gram-Schmidt run twice, three passes over the basis
     GsArgs<TB> g;
@@ -699,6 +734,37 @@ int a2d_plan_workspace_bytes(const a2d_plan* P, size_t* bytes) {
 
 int a2d_plan_ncases(const a2d_plan* P) { return P ? P->ncases : 0; }
 
+int a2d_plan_set_tuning(a2d_plan* P, int jvp_tile, int sweep_variant, void* stream) {
+  if (P == nullptr) return fail(A2D_ERR_ARG, "null plan");
+  if (jvp_tile < 0 || jvp_tile >= kNumTileShapes) return fail(A2D_ERR_ARG, "set_tuning: unknown JVP tile shape");
+  if (sweep_variant < 0 || sweep_variant >= kNumSweepVariants)
+    return fail(A2D_ERR_ARG, "set_tuning: unknown sweep variant");
+  if (jvp_tile != P->jvp_tile) {
+    P->jvp_tile = jvp_tile;
+    P->jtiles = tile_list(P, jvp_tile);
+    if (P->ws != nullptr) {
+      cudaStream_t s = static_cast<cudaStream_t>(stream);
+      A2D_CK(cudaMemcpyAsync(P->ws + P->o_jtiles, P->jtiles.data(), sizeof(Tile) * P->jtiles.size(),
+                             cudaMemcpyHostToDevice, s));
+      A2D_CK(cudaStreamSynchronize(s));
+      P->jbatch.ntiles = (int)P->jtiles.size();
+    }
+  }
+  P->sweep_variant = sweep_variant;
+  if (P->graph != nullptr) {   // the captured step holds the old launch configuration
+    cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+  }
+  return A2D_OK;
+}
+
+int a2d_plan_get_tuning(const a2d_plan* P, int* jvp_tile, int* sweep_variant) {
+  if (P == nullptr) return fail(A2D_ERR_ARG, "null plan");
+  if (jvp_tile != nullptr) *jvp_tile = P->jvp_tile;
+  if (sweep_variant != nullptr) *sweep_variant = P->sweep_variant;
+  return A2D_OK;
+}
+
 int a2d_plan_bind(a2d_plan* P, void* workspace, size_t bytes, void* stream) {
   if (P == nullptr || workspace == nullptr) return fail(A2D_ERR_ARG, "bind: null argument");
   if (bytes < P->bytes) return fail(A2D_ERR_ARG, "bind: workspace too small");
@@ -730,11 +796,18 @@ int a2d_plan_bind(a2d_plan* P, void* workspace, size_t bytes, void* stream) {
   B.ntiles = (int)P->tiles.size();
   B.nchunks = (int)P->chunks.size();
   B.ngroups = (int)P->groups.size();
+  A2D_CK(cudaMemcpyAsync(P->ws + P->o_jtiles, P->jtiles.data(), sizeof(Tile) * P->jtiles.size(),
+                         cudaMemcpyHostToDevice, s));
+  P->jbatch = B;
+  P->jbatch.tiles = P->at<Tile>(P->o_jtiles);
+  P->jbatch.ntiles = (int)P->jtiles.size();
   if (P->host_count == nullptr) A2D_CK(cudaMallocHost(&P->host_count, 2 * sizeof(int)));
   A2D_CK(cudaMemsetAsync(P->ws + P->o_cnt, 0, 8, s));
   A2D_CK(cudaMemsetAsync(P->ws + P->o_sat, 0, sizeof(unsigned long long), s));
   A2D_CK(sweep_init());
   A2D_CK(gs_init());
+  stencil_init_fp64();
+  stencil_init_fp32();
   k_reset<<<(P->ncases + 63) / 64, 64, 0, s>>>(P->ncases, P->ctl(), P->live(), P->p.cfl0);
   A2D_CK(cudaMemsetAsync(P->ws + P->o_circ_rk, 0, 8 * (size_t)P->ncases, s));
   A2D_CK(cudaGetLastError());
@@ -906,8 +979,13 @@ int a2d_jvp(a2d_plan* P, void* stream) {
   a.out = P->vec(kJV);
   Batch B = P->batch;
   B.live = nullptr;
-  if (P->p.precision == A2D_MIXED) launch_stencil<float, true, double>(B, a, static_cast<cudaStream_t>(stream));
-  else launch_stencil<double, true, double>(B, a, static_cast<cudaStream_t>(stream));
+  if (P->p.precision == A2D_MIXED) {
+    Batch jb = P->jbatch;
+    jb.live = nullptr;
+    launch_stencil<float, true, double>(jb, a, static_cast<cudaStream_t>(stream), P->jvp_tile);
+  } else {
+    launch_stencil<double, true, double>(B, a, static_cast<cudaStream_t>(stream));
+  }
   A2D_CK(cudaGetLastError());
   return A2D_OK;
 }
@@ -1049,7 +1127,9 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
           a.lim_k = P->p.lim_k;
           a.order = P->p.order;
           a.vortex = P->p.vortex_correction;
-          launch_stencil<float, true, Basis16>(B, a, s);
+          Batch jb = P->jbatch;
+          jb.live = nullptr;
+          launch_stencil<float, true, Basis16>(jb, a, s, P->jvp_tile);
         } else {
           StencilArgs<double> a = residual_args(P);
           a.V = P->at<double>(P->o_V);
@@ -1064,8 +1144,8 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
         a.e0 = P->vec(kPE);
         a.xprev = P->vec(kPB);
         a.x = P->vec(kPA);
-        if (mixed) launch_sweep<float, false>(B, a, false, s);
-        else launch_sweep<double, false>(B, a, false, s);
+        if (mixed) launch_sweep<float, false>(B, a, false, s, P->sweep_variant);
+        else launch_sweep<double, false>(B, a, false, s, P->sweep_variant);
         break;
       }
       case A2D_K_SWEEP_FIRST: {
@@ -1073,8 +1153,8 @@ int a2d_time_kernel(a2d_plan* P, int which, int reps, float* ms, void* stream) {
         a.r = P->vec(kZ);
         a.e0 = P->vec(kPE);
         a.x = P->vec(kPA);
-        if (mixed) launch_sweep<float, true>(B, a, false, s);
-        else launch_sweep<double, true>(B, a, false, s);
+        if (mixed) launch_sweep<float, true>(B, a, false, s, P->sweep_variant);
+        else launch_sweep<double, true>(B, a, false, s, P->sweep_variant);
         break;
       }
       case A2D_K_DOTS:
@@ -1222,7 +1302,7 @@ int a2d_smooth(a2d_plan* P, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   Batch B = P->batch;
   B.live = nullptr;
-  launch_irs(B, P->vec(kR), P->vec(kPA), P->p.irs_eps, P->max_ni, P->max_nc, s);
+  launch_irs(B, P->vec(kR), P->vec(kPA), P->p.irs_eps, P->max_ni, P->max_nc, P->p.precision == A2D_MIXED, s);
   if (P->p.irs_eps > 0)
     A2D_CK(cudaMemcpyAsync(P->vec(kR), P->vec(kPA), 8 * 4 * (size_t)P->C, cudaMemcpyDeviceToDevice, s));
   A2D_CK(cudaGetLastError());
@@ -1261,21 +1341,26 @@ static cudaError_t rk_iter(a2d_plan* P, const double* circ, const double* forcin
   double* Rs = P->vec(kPA);
   double* dt = P->at<double>(P->o_dt);
   const double alphas[4] = {0.25, 1.0 / 3.0, 0.5, 1.0};
+  // dtype=float32: residual, local time steps, smoothing and stage update in FP32
+  // (the reference casts its whole explicit iteration to the solver dtype,
+  // aero2d/euler.py:222-234); the state keeps FP32-rounded values in FP64 storage
+  const bool fp32 = P->p.precision == A2D_MIXED;
   if (cudaError_t e = cudaMemcpyAsync(U0, U, 8 * 4 * (size_t)P->C, cudaMemcpyDeviceToDevice, s)) return e;
-  launch_local_dt(B, U, dt, P->p.cfl, s);
+  launch_local_dt(B, U, dt, P->p.cfl, fp32, s);
   for (int st = 0; st < 4; ++st) {
     StencilArgs<double> a = residual_args(P);
     a.circ_in = circ;
     a.out = R;
     a.sign = 1.0;
-    launch_stencil<double, false, double>(B, a, s);
+    if (fp32) launch_stencil<float, false, double>(B, a, s);
+    else launch_stencil<double, false, double>(B, a, s);
     if (forcing != nullptr) launch_add_forcing(B, R, forcing, s);
     const double* Ruse = R;
     if (P->p.irs_eps > 0) {
-      launch_irs(B, R, Rs, P->p.irs_eps, P->max_ni, P->max_nc, s);
+      launch_irs(B, R, Rs, P->p.irs_eps, P->max_ni, P->max_nc, fp32, s);
       Ruse = Rs;
     }
-    launch_rk_stage(B, U0, Ruse, dt, U, alphas[st], s);
+    launch_rk_stage(B, U0, Ruse, dt, U, alphas[st], fp32, s);
   }
   return cudaGetLastError();
 }
@@ -1296,7 +1381,8 @@ static cudaError_t fas_cycle(a2d_plan* P, const double* circ, const double* forc
   a.circ_in = circ;
   a.out = P->vec(kR);
   a.sign = 1.0;
-  launch_stencil<double, false, double>(B, a, s);
+  if (P->p.precision == A2D_MIXED) launch_stencil<float, false, double>(B, a, s);
+  else launch_stencil<double, false, double>(B, a, s);
   if (forcing != nullptr) launch_add_forcing(B, P->vec(kR), forcing, s);
   // coarse start state Uc0 (kept in the coarse plan's JV slot) and forcing (its V slot)
   double* Uc = Cp->vec(kU);
@@ -1307,7 +1393,8 @@ static cudaError_t fas_cycle(a2d_plan* P, const double* circ, const double* forc
   ca.circ_in = circ;
   ca.out = Pc;
   ca.sign = 1.0;
-  launch_stencil<double, false, double>(CB, ca, s);
+  if (Cp->p.precision == A2D_MIXED) launch_stencil<float, false, double>(CB, ca, s);
+  else launch_stencil<double, false, double>(CB, ca, s);
   launch_fas_forcing(B, CB, P->vec(kR), Pc, s);
   if (cudaError_t e = fas_cycle(Cp, circ, Pc, false, s)) return e;
   launch_fas_prolong(B, CB, P->vec(kU), Uc, Uc0, s);

@@ -50,6 +50,7 @@ struct a2d_service {
     std::vector<double> coef;       // [npts][3]
     std::vector<double> cp;         // [npts][ni]
     std::vector<int> converged, nsteps;
+    std::vector<double> drop;       // [npts] last finite residual norm / r0
   };
   std::map<long long, Request> reqs;
   std::deque<long long> queue;
@@ -61,6 +62,7 @@ struct a2d_service {
   std::vector<long long> finished;       // finished since the last poll
   long long next_id = 1;
   long long total_ni = 0;
+  long long newton_steps = 0;            // Newton steps taken by the plan since bind
   std::mutex mu;
 };
 
@@ -87,6 +89,7 @@ int submit(a2d_service* S, int cls, const void* metrics, int npoints, const doub
   r.cp.assign((size_t)npoints * ni, 0.0);
   r.converged.assign(npoints, 0);
   r.nsteps.assign(npoints, 0);
+  r.drop.assign(npoints, NAN);
   std::lock_guard<std::mutex> lk(S->mu);
   const long long rid = S->next_id++;
   S->reqs.emplace(rid, std::move(r));
@@ -227,6 +230,7 @@ int a2d_service_step(a2d_service* S, int* busy, void* stream) {
   if (nbusy == 0) return A2D_OK;
 
   if (int e = a2d_newton_step(S->plan, stream)) return e;
+  S->newton_steps += 1;
   std::vector<int> nsteps(S->slots), done(S->slots), frozen(S->slots);
   std::vector<double> lastrn(S->slots), r0(S->slots);
   if (int e = a2d_case_status(S->plan, nsteps.data(), done.data(), frozen.data(), lastrn.data(), r0.data(), stream))
@@ -251,6 +255,7 @@ int a2d_service_step(a2d_service* S, int* busy, void* stream) {
     // the reference's flag (aero2d/implicit.py:252): not frozen and three orders down
     r.converged[pt] = !frozen[k] && std::isfinite(lastrn[k]) && lastrn[k] < 1e-3 * r0[k];
     r.nsteps[pt] = nsteps[k];
+    r.drop[pt] = lastrn[k] / r0[k];
     r.done_pts += 1;
     if (r.next < r.npts) {
       const int np = r.next++;
@@ -314,6 +319,17 @@ int a2d_service_result(a2d_service* S, long long id, double* coef, double* cp, i
   return A2D_OK;
 }
 
+int a2d_service_result_drop(a2d_service* S, long long id, double* drop) {
+  if (S == nullptr || drop == nullptr) return fail(A2D_ERR_ARG, "service_result_drop: bad arguments");
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(id);
+  if (it == S->reqs.end()) return fail(A2D_ERR_ARG, "service_result_drop: unknown request");
+  const a2d_service::Request& r = it->second;
+  if (r.done_pts < r.npts) return fail(A2D_ERR_STATE, "service_result_drop: request not finished");
+  std::copy(r.drop.begin(), r.drop.end(), drop);
+  return A2D_OK;
+}
+
 int a2d_service_pending(a2d_service* S, int* queued, int* running) {
   if (S == nullptr) return fail(A2D_ERR_ARG, "null service");
   std::lock_guard<std::mutex> lk(S->mu);
@@ -324,6 +340,19 @@ int a2d_service_pending(a2d_service* S, int* queued, int* running) {
     *running = nb;
   }
   return A2D_OK;
+}
+
+int a2d_service_plan(a2d_service* S, a2d_plan** plan) {
+  if (S == nullptr || plan == nullptr) return fail(A2D_ERR_ARG, "service_plan: bad arguments");
+  *plan = S->plan;
+  return A2D_OK;
+}
+
+int a2d_service_stats(a2d_service* S, int* kernels_per_step, long long* newton_steps) {
+  if (S == nullptr) return fail(A2D_ERR_ARG, "null service");
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (newton_steps != nullptr) *newton_steps = S->newton_steps;
+  return a2d_plan_stats(S->plan, kernels_per_step, nullptr, nullptr);
 }
 
 int a2d_service_destroy(a2d_service* S) {

@@ -137,8 +137,13 @@ void launch_metrics(int ni, int nc, const double* x, const double* y, double* md
   k_metrics<<<blocks, 256, 0, s>>>(ni, nc, x, y, md, mf);
 }
 
-template void launch_stencil<double, false, double>(const Batch&, const StencilArgs<double>&, cudaStream_t);
-template void launch_stencil<double, true, double>(const Batch&, const StencilArgs<double>&, cudaStream_t);
+template void launch_stencil<double, false, double>(const Batch&, const StencilArgs<double>&, cudaStream_t, int);
+template void launch_stencil<double, true, double>(const Batch&, const StencilArgs<double>&, cudaStream_t, int);
+
+void stencil_init_fp64() {
+  stencil_cap<double, false, double, kTI, kTJ>();
+  stencil_cap<double, true, double, kTI, kTJ>();
+}
 
 void launch_forces(const Batch& b, const double* U, double* coef, double* cp, const long long* cp_off,
                    const CaseCtl* ctl, double* hist_cl, int hist_cap, cudaStream_t s) {

@@ -11,10 +11,26 @@
 
 namespace a2d {
 
-template void launch_stencil<float, false, double>(const Batch&, const StencilArgs<double>&, cudaStream_t);
-template void launch_stencil<float, true, double>(const Batch&, const StencilArgs<double>&, cudaStream_t);
-template void launch_stencil<float, true, float>(const Batch&, const StencilArgs<float>&, cudaStream_t);
+template void launch_stencil<float, false, double>(const Batch&, const StencilArgs<double>&, cudaStream_t, int);
+template void launch_stencil<float, true, double>(const Batch&, const StencilArgs<double>&, cudaStream_t, int);
+template void launch_stencil<float, true, float>(const Batch&, const StencilArgs<float>&, cudaStream_t, int);
 template void launch_stencil<float, true, __nv_bfloat16>(const Batch&, const StencilArgs<__nv_bfloat16>&,
-                                                         cudaStream_t);
+                                                         cudaStream_t, int);
+
+
+template <typename VT>
+static void caps_of() {
+  stencil_cap<float, true, VT, kTI, kTJ>();
+  stencil_cap<float, true, VT, 32, 16>();
+  stencil_cap<float, true, VT, 64, 4>();
+  stencil_cap<float, true, VT, 16, 16>();
+}
+
+void stencil_init_fp32() {
+  stencil_cap<float, false, double, kTI, kTJ>();
+  caps_of<double>();
+  caps_of<float>();
+  caps_of<__nv_bfloat16>();
+}
 
 }  // namespace a2d

@@ -119,17 +119,17 @@ __device__ void block_circulation(const CaseDev& cs, const double* U, const VT* 
 // ---------------------------------------------------------------------------
 // the fused residual / JVP tile kernel
 // ---------------------------------------------------------------------------
-template <typename T, bool LIN, typename VT>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_stencil(Batch b, StencilArgs<VT> a) {
+template <typename T, bool LIN, typename VT, int TI, int TJ>
+__device__ __forceinline__ void stencil_tile(const Batch& b, const StencilArgs<VT>& a, int tile) {
   using S = typename std::conditional<LIN, Dual<T, 1>, T>::type;
-  constexpr int WI = kTI + 4, WJ = kTJ + 4;
+  constexpr int WI = TI + 4, WJ = TJ + 4;
   __shared__ S sW[4][WJ][WI];
-  __shared__ T sFi[4][kTJ][kTI + 1];
-  __shared__ T sFj[4][kTJ + 1][kTI];
+  __shared__ T sFi[4][TJ][TI + 1];
+  __shared__ T sFj[4][TJ + 1][TI];
   __shared__ T sred[32 * 4];
   __shared__ T sGam[2];
 
-  const Tile t = b.tiles[blockIdx.x];
+  const Tile t = b.tiles[tile];
   if (!case_live(b, t.cs, a.need)) return;
   const CaseDev cs = b.cases[t.cs];
   const GridDev& g = cs.g;
@@ -293,15 +293,62 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_stencil(Batch b
       double v[1] = {part};
       __shared__ double sredd[32];
       block_sum<double, 1>(v, sredd);
-      if (threadIdx.x == 0) a.tile_part[(size_t)blockIdx.x * kTilePartStride] = v[0];
+      if (threadIdx.x == 0) a.tile_part[(size_t)tile * kTilePartStride] = v[0];
     }
   }
 }
 
+// Persistent: the grid is at most the CTAs resident on the GPU, and each CTA
+// walks the batch's tile list (every case's tiles, whatever their grid size)
+// with a stride of the grid size.  TI x TJ is the tile shape of that list.
+template <typename T, bool LIN, typename VT, int TI, int TJ>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_stencil(Batch b, StencilArgs<VT> a) {
+  for (int tile = blockIdx.x; tile < b.ntiles; tile += gridDim.x) {
+    if (tile != (int)blockIdx.x) __syncthreads();   // the previous tile is done with shared memory
+    stencil_tile<T, LIN, VT, TI, TJ>(b, a, tile);
+  }
+}
+
+// CTAs of a persistent stencil launch: the tiles, at most the CTAs of kernel f
+// resident at once on the current device (its occupancy times the SMs)
+inline int persistent_grid(const void* f, int threads, int items) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+    sms = 148;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, threads, 0) != cudaSuccess || per_sm <= 0)
+    per_sm = 1;
+  const long long cap = (long long)sms * per_sm;
+  return items < cap ? items : (int)cap;
+}
+
+// resident CTAs of one instantiation, queried once (stencil_init_fp64/_fp32 at
+// plan bind, so that no query runs while a Newton step is being captured)
+template <typename T, bool LIN, typename VT, int TI, int TJ>
+int stencil_cap() {
+  static int cap = 0;
+  if (cap == 0) cap = persistent_grid(reinterpret_cast<const void*>(&k_stencil<T, LIN, VT, TI, TJ>), 256, 1 << 30);
+  return cap;
+}
+
+template <typename T, bool LIN, typename VT, int TI, int TJ>
+void launch_stencil_shape(const Batch& b, const StencilArgs<VT>& a, cudaStream_t s) {
+  const int cap = stencil_cap<T, LIN, VT, TI, TJ>();
+  k_stencil<T, LIN, VT, TI, TJ><<<b.ntiles < cap ? b.ntiles : cap, 256, 0, s>>>(b, a);
+}
+
 template <typename T, bool LIN, typename VT>
-void launch_stencil(const Batch& b, const StencilArgs<VT>& a, cudaStream_t s) {
+void launch_stencil(const Batch& b, const StencilArgs<VT>& a, cudaStream_t s, int shape) {
   if (b.ntiles == 0) return;
-  k_stencil<T, LIN, VT><<<b.ntiles, 256, 0, s>>>(b, a);
+  if constexpr (LIN && sizeof(T) == 4) {
+    switch (shape) {
+      case kTile32x16: launch_stencil_shape<T, LIN, VT, 32, 16>(b, a, s); return;
+      case kTile64x4: launch_stencil_shape<T, LIN, VT, 64, 4>(b, a, s); return;
+      case kTile16x16: launch_stencil_shape<T, LIN, VT, 16, 16>(b, a, s); return;
+      default: break;
+    }
+  }
+  launch_stencil_shape<T, LIN, VT, kTI, kTJ>(b, a, s);
 }
 
 }  // namespace a2d

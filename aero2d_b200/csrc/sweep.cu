@@ -15,30 +15,30 @@
 // + JIR(i+1) x'[i+1]); eliminating from both ends halves the sequential depth
 // of a line from 2 nc to about nc dependent steps.
 //
-// One CTA of nine warps per 32-line group, warp-specialised.  Warps 0-3 solve
-// the wall half and warps 4-7 the far-field half, in parallel (lane = line,
-// warp = row of the 4x4 blocks); warp 8 is the producer: for every step of each
-// half its lane 0 brings the step's blocks by TMA bulk copies (one contiguous
-// run per row: fbidx/fbidx3, a consumer's block row is one vector load) into a
-// ring of kStages stages per half with two mbarriers per stage: "full" (the
-// bulk-copy bytes) and "empty" (one arrival per consumer warp that is done with
-// the stage).  Each consumer thread loads its own vector entries of the forward
-// steps (component q of its line) through L2 into registers kAhead steps ahead
-// and stores them into a two-slot shared buffer the step before they are used,
-// so that the step's barrier publishes them to the other row warps; a line's
-// 4-vector passes between the four row warps of a half through a two-slot
-// exchange buffer, one named barrier per step, and the halves meet twice
-// around the twist row.  (Per-thread L1-allocating cp.async copies of the
-// vectors written by the preceding sweep were measured to return stale data
-// now and then, so these loads bypass L1.)  d_j goes to x (the last sweep, whose
-// x is FP64: to a scratch vector) and comes back, register-prefetched, in the
-// back substitution.  Every wait is bounded; a wait that runs out records an
-// error and the CTA drains its copies in flight (bounded again) before exit.
+// One CTA of two warps per 32-line group: warp 0 solves the wall half and
+// warp 1 the far-field half, in parallel; each lane owns one line and all four
+// rows of its 4x4 blocks, so a step needs no barrier: the recurrence's 4-vector
+// stays in the lane's registers.  Each warp streams its own factor blocks: lane
+// 0 keeps kStages steps in flight, one TMA bulk copy per factor run (a group's
+// blocks of one row are one contiguous run: fbidx/fbidx3, a lane's block row is
+// one vector load) into a ring of kStages stages, each with one mbarrier that
+// counts the copy's bytes; once the warp is done with a stage, lane 0 refills
+// it with the step kStages ahead.  Each lane loads its line's vector entries
+// (r, or e0 and x' of both neighbour lines) through L2 into registers kAhead
+// steps before their use (the vectors written by the preceding sweep bypass
+// L1).  The halves meet at the twist row through shared memory, two named
+// barriers of the CTA's 64 threads.  d_j goes to x (the last sweep, whose x is
+// FP64: to a scratch vector) and comes back, register-prefetched, in the back
+// substitution.  Every wait is bounded; a wait that runs out records an error,
+// both warps still meet at both barriers, and each drains the copies it issued
+// (bounded again) before it exits.
 //
 // Arithmetic and intermediate vectors are in the sweep's compute type: FP64
 // in the FP64 path; FP32 in the mixed path, whose factors are FP16 and pivot
 // inverses FP32 (a preconditioner only steers GMRES; the Newton residual and
-// the Krylov reductions stay FP64).
+// the Krylov reductions stay FP64).  The operation order of every row is fixed
+// (products summed over the columns in order), so results are bitwise
+// repeatable.
 #include <type_traits>
 
 #include "batch.cuh"
@@ -47,12 +47,8 @@
 
 namespace a2d {
 
-constexpr int kHalfThreads = 128;                       // consumer threads of one half
-constexpr int kConsumerThreads = 2 * kHalfThreads;
-constexpr int kProducerWarp = kConsumerThreads / 32;    // warp 8
-constexpr int kSweepThreads = kConsumerThreads + 32;
+constexpr int kSweepThreads = 64;                       // warp 0: wall half, warp 1: far-field half
 constexpr int kBlockEntries = 16 * kLanes;              // one 4x4 block for the 32 lines of a group
-constexpr int kBackAhead = 8;                           // register prefetch depth of d in the back substitution
 
 // TI: pivot inverses (the Jacobian type); TF: the other factors (FactorStore);
 // TC: arithmetic and intermediate vectors
@@ -60,14 +56,16 @@ template <typename TI> struct SweepTypes;
 template <> struct SweepTypes<float> {
   using TF = __half;
   using TC = float;
-  static constexpr int kStages = 4;   // bulk-copy ring stages per half
-  static constexpr int kAhead = 2;    // steps between loading a vector entry and its use
+  static constexpr int kStages = 6;     // bulk-copy ring stages per half
+  static constexpr int kAhead = 4;      // steps between loading a vector entry and its use
+  static constexpr int kBackAhead = 8;  // register prefetch depth of d in the back substitution
 };
 template <> struct SweepTypes<double> {
   using TF = double;
   using TC = double;
   static constexpr int kStages = 2;
   static constexpr int kAhead = 2;
+  static constexpr int kBackAhead = 4;
 };
 
 template <typename TI>
@@ -79,17 +77,11 @@ struct SweepSmem {
   static constexpr uint32_t kBytesF = kBlockEntries * sizeof(TF);
   // the twist step carries the most: (INV, G, H) or (P, Q, G, H)
   static constexpr uint32_t kMatBytes = (kBytesI + 2 * kBytesF > 4 * kBytesF) ? kBytesI + 2 * kBytesF : 4 * kBytesF;
-  // forward: r (FP64) or (e0, x'[i-1], x'[i+1]) in TC, each [line][component]
-  static constexpr uint32_t kVecBytes =
-      (3 * kLanes * 4 * sizeof(TC) > kLanes * 4 * sizeof(double)) ? 3 * kLanes * 4 * sizeof(TC)
-                                                                   : kLanes * 4 * sizeof(double);
   alignas(128) unsigned char mat[2][kS][kMatBytes];
-  alignas(16) unsigned char vec[2][2][kVecBytes];   // per half, by step parity
-  alignas(16) TC xchg[2][2][kLanes][4];   // per half: the previous step's 4-vector of every line
+  alignas(16) TC dk[kLanes][4];           // the far-field half's d'_{k+1}
   alignas(16) TC xk[kLanes][4];           // the twist row's solution
   uint64_t full[2][kS];
-  uint64_t empty[2][kS];
-  int failed[2];                          // per half: stopped early
+  int failed[2];                          // per half: a wait ran out
 };
 
 // the four entries of one block row of one line, converted to the compute type
@@ -103,43 +95,20 @@ __device__ __forceinline__ void load4(const float* p, float (&v)[4]) {
   const float4 t = *reinterpret_cast<const float4*>(p);
   v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
 }
-__device__ __forceinline__ void load4(const double* p, float (&v)[4]) {
-  const double2 t0 = *reinterpret_cast<const double2*>(p);
-  const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
-  v[0] = (float)t0.x; v[1] = (float)t0.y; v[2] = (float)t1.x; v[3] = (float)t1.y;
-}
 __device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
   const double2 t0 = *reinterpret_cast<const double2*>(p);
   const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
   v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
 }
 
-// barrier of the 128 consumer threads of one half (ids 1, 2) and of all 256
-// consumer threads (id 3); the producer warp takes part in none
-__device__ __forceinline__ void half_sync(int h) {
-  asm volatile("bar.sync %0, %1;" ::"r"(1 + h), "r"(kHalfThreads) : "memory");
-}
-// the same barrier of one half, OR-reducing a per-thread flag over its 128 threads
-__device__ __forceinline__ bool half_sync_or(int h, bool flag) {
-  uint32_t r;
-  asm volatile(
-      "{\n"
-      " .reg .pred pi, po;\n"
-      " setp.ne.u32 pi, %1, 0;\n"
-      " bar.red.or.pred po, %2, %3, pi;\n"
-      " selp.u32 %0, 1, 0, po;\n"
-      "}\n"
-      : "=r"(r)
-      : "r"((uint32_t)flag), "r"(1 + h), "r"(kHalfThreads)
-      : "memory");
-  return r != 0;
-}
-__device__ __forceinline__ void consumers_sync() {
-  asm volatile("bar.sync 3, %0;" ::"r"(kConsumerThreads) : "memory");
-}
+// the 64 threads of the CTA (named barrier 1)
+__device__ __forceinline__ void halves_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kSweepThreads) : "memory"); }
+
+// orders this warp's reads of a ring stage before the bulk copy that refills it
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 template <typename TI, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a) {
+__global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   using SM = SweepSmem<TI>;
   using TF = typename SM::TF;
   using TC = typename SM::TC;
@@ -150,333 +119,328 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   constexpr uint32_t kBytesI = SM::kBytesI, kBytesF = SM::kBytesF;
   constexpr uint32_t kOffG = FIRST ? kBytesI : 2 * kBytesF;   // G's block in a forward stage
   constexpr uint32_t kOffH = kOffG + kBytesF;                // H's block in the twist stage
+  constexpr int L = SweepTypes<TI>::kAhead;   // at most 4 (the twist's slot switch below)
+  static_assert(L >= 1 && L <= 4, "kAhead must be in [1, 4]");
+  constexpr int LB = SweepTypes<TI>::kBackAhead;
 
   const Group grp = b.groups[blockIdx.x];
   if (!case_live(b, grp.cs, a.need)) return;
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5, lane = tid & 31;
+  const int h = threadIdx.x >> 5;              // 0: from the wall, 1: from the far field
+  const int l = threadIdx.x & 31;              // line within the group
   const CaseDev cs = b.cases[grp.cs];
   const int ni = cs.g.ni, nc = cs.g.nc;
   const int k = nc / 2;                        // twist row (as in k_factor)
   const int nf0 = k, nf1 = nc - 1 - k;         // forward steps of the wall / far-field half
-  const int ns0 = 2 * k + 1, ns1 = 2 * nf1;    // steps of each half
-  // step t of half h: forward rows first; the wall half's step k is the twist
+  const int nf = h == 0 ? nf0 : nf1;
+  const int nsteps = h == 0 ? 2 * k + 1 : 2 * nf1;
+  // step t of the half: forward rows first; the wall half's step k is the twist
   // row; then the back substitution outward from the twist row
-  auto row_of = [&](int h, int t) {
+  auto row_of = [&](int t) {
     if (h == 0) return t <= k ? t : 2 * k - t;
     return t < nf1 ? nc - 1 - t : k + 1 + (t - nf1);
   };
-  const size_t vbase = 4 * (size_t)cs.cell_off;
-  const size_t comp = (size_t)nc * ni;         // stride between the components of a case vector
   const size_t blk0 = lbidx(cs.rows_nc, nc, grp.g, 0, 0, 0);   // row j's block at blk0 + j * kBlockEntries
 
-  if (tid == 0) {
+  if (l == 0) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-#pragma unroll
-      for (int s = 0; s < S; ++s) {
-        mbar_init(&sm.full[h][s], 1);        // the producer's arrival with the bulk-copy bytes
-        mbar_init(&sm.empty[h][s], 4);       // one arrival per consumer warp of the half
-      }
-      sm.failed[h] = 0;
-    }
+    for (int s = 0; s < S; ++s) mbar_init(&sm.full[h][s], 1);   // lane 0's arrival with the copy's bytes
+    sm.failed[h] = 0;
     mbar_init_fence();
-  }
-  if (warp < kProducerWarp) {
-    const int h = warp >> 2, q = warp & 3;
-    sm.xchg[h][0][lane][q] = TC(0);
-    sm.xchg[h][1][lane][q] = TC(0);   // d_{-1} = d'_{nc} = 0
   }
   __syncthreads();
 
-  // ======================= producer warp =======================
-  if (warp == kProducerWarp) {
-    const TI* INV = static_cast<const TI*>(a.INV);
-    const TF* PQG = static_cast<const TF*>(a.PQG);
-    const TF* CF = static_cast<const TF*>(a.CF);
-    int issued[2] = {0, 0};
-    bool ok = true;
-    const int smax = ns0 > ns1 ? ns0 : ns1;
-#pragma unroll 1
-    for (int t = 0; t < smax && ok; ++t) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (!ok || t >= (h == 0 ? ns0 : ns1)) continue;
-        const int s = t % S;
-        if (t >= S && !mbar_wait(&sm.empty[h][s], ((t / S) - 1) & 1)) {
-          ok = false;
-          continue;
-        }
-        const int j = row_of(h, t);
-        const bool twist = h == 0 && t == k;
-        const bool fwd = twist || t < (h == 0 ? nf0 : nf1);
-        uint64_t* bar = &sm.full[h][s];
-        if (lane == 0) {
-          unsigned char* m = sm.mat[h][s];
-          const size_t o = blk0 + (size_t)j * kBlockEntries;
-          if (fwd) {
-            if constexpr (FIRST) {
-              mbar_arrive_expect(bar, kBytesI + (twist ? 2 : 1) * kBytesF);
-              bulk_load(m, INV + o, kBytesI, bar);
-              bulk_load(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, bar);
-              if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
-            } else {
-              mbar_arrive_expect(bar, (twist ? 4 : 3) * kBytesF);
-              bulk_load(m, PQG + 3 * o, 3 * kBytesF, bar);   // P, Q, G: one run
-              if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
-            }
-          } else {
-            mbar_arrive_expect(bar, kBytesF);
-            bulk_load(m, CF + o, kBytesF, bar);
-          }
-        }
-        issued[h] = t + 1;
+  // lane 0: bulk copies of step t's factor blocks into stage t % S
+  const TI* INV = static_cast<const TI*>(a.INV);
+  const TF* PQG = static_cast<const TF*>(a.PQG);
+  const TF* CF = static_cast<const TF*>(a.CF);
+  int issued = 0;
+  auto issue = [&](int t) {
+    const int j = row_of(t);
+    const bool twist = h == 0 && t == k;
+    const bool fwd = twist || t < nf;
+    uint64_t* bar = &sm.full[h][t % S];
+    unsigned char* m = sm.mat[h][t % S];
+    const size_t o = blk0 + (size_t)j * kBlockEntries;
+    if (fwd) {
+      if constexpr (FIRST) {
+        mbar_arrive_expect(bar, kBytesI + (twist ? 2 : 1) * kBytesF);
+        bulk_load(m, INV + o, kBytesI, bar);
+        bulk_load(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, bar);
+        if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
+      } else {
+        mbar_arrive_expect(bar, (twist ? 4 : 3) * kBytesF);
+        bulk_load(m, PQG + 3 * o, 3 * kBytesF, bar);   // P, Q, G: one run
+        if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
       }
+    } else {
+      mbar_arrive_expect(bar, kBytesF);
+      bulk_load(m, CF + o, kBytesF, bar);
     }
-    if (!ok) {
-      // the consumers stopped: record it, and give the copies still in flight
-      // a bounded time to land before the CTA's shared memory goes away
-      if (lane == 0 && a.err != nullptr) atomicExch(a.err, 1u);
-#pragma unroll 1
-      for (int h = 0; h < 2; ++h)
-        for (int u = issued[h] > S ? issued[h] - S : 0; u < issued[h]; ++u)
-          (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
+  };
+  if (l == 0)
+    for (; issued < S && issued < nsteps; ++issued) issue(issued);
+  // the warp is done with stage t: lane 0 refills it with step t + S
+  auto advance = [&](int t) {
+    __syncwarp();
+    if (l == 0 && issued < nsteps) {
+      fence_proxy_async();
+      issue(issued);
+      ++issued;
     }
-    return;
-  }
+  };
+  // waits for step t's stage; false (on every lane) once any lane's wait ran out
+  auto wait_full = [&](int t) -> bool {
+    const bool ok = mbar_wait(&sm.full[h][t % S], (t / S) & 1);
+    return __all_sync(0xffffffffu, ok);
+  };
 
-  // ======================= consumers =======================
-  const int h = warp >> 2;                     // 0: from the wall, 1: from the far field
-  const int q = warp & 3;                      // row of the blocks owned by this warp
-  const int l = lane;                          // line within the group
   const bool owner = l < grp.n;                // lanes past the group's last line only compute
   const int i = grp.i0 + (owner ? l : grp.n - 1);
   const int im = (i == 0) ? ni - 1 : i - 1;
   const int ip = (i + 1 == ni) ? 0 : i + 1;
-  const int nf = h == 0 ? nf0 : nf1;
-  const int nsteps = h == 0 ? ns0 : ns1;
-  const size_t vq = vbase + (size_t)q * comp;  // component q of the case's vectors
-  TX* x = reinterpret_cast<TX*>(a.x) + vq;
+  const size_t vbase = 4 * (size_t)cs.cell_off;
+  const size_t comp = (size_t)nc * ni;         // stride between the components of a case vector
+  // per-line bases: row offsets within a component plane stay 32-bit
+  const TC* e0b = reinterpret_cast<const TC*>(a.e0) + vbase + i;
+  const TC* xmb = reinterpret_cast<const TC*>(a.xprev) + vbase + im;
+  const TC* xpb = reinterpret_cast<const TC*>(a.xprev) + vbase + ip;
+  const double* rb = a.r + vbase + i;
+  TC* e0w = reinterpret_cast<TC*>(a.e0) + vbase + i;
   // d_j in the compute type: in x itself, or (last sweep, FP64 x) in the scratch
-  TC* dv = reinterpret_cast<TC*>(LAST ? a.dtmp : a.x) + vq;
-  const int eo = (q * kLanes + l) * 4;         // this thread's entries in a block
-  const TC* e0v = reinterpret_cast<const TC*>(a.e0) + vq;
-  const TC* xpv = reinterpret_cast<const TC*>(a.xprev) + vq;
-  const double* rv = a.r + vq;
-
-  // rows as offsets into a component plane: forward step t of the half is row
-  // jf0 + t * jdir (the wall half's twist row k continues the sequence); the
-  // back substitution runs outward from the twist row
+  TC* dvb = reinterpret_cast<TC*>(LAST ? a.dtmp : a.x) + vbase + i;
+  TX* xb = reinterpret_cast<TX*>(a.x) + vbase + i;
+  const int eo = l * 4;                        // this lane's entries in block row r: eo + r * kLanes * 4
   const int rstep = h == 0 ? ni : -ni;
   const int rf0 = h == 0 ? 0 : (nc - 1) * ni;
-  // per-thread bases: offsets within a component plane stay 32-bit
-  const TC* e0b = e0v + i;
-  const TC* xmb = xpv + im;
-  const TC* xpb = xpv + ip;
-  const double* rb = rv + i;
-  TC* dvb = dv + i;
-  TX* xb = x + i;
   const int nvec = h == 0 ? k + 1 : nf1;       // steps with vector entries (forward, and the twist)
 
-  // the vector entries of step u: each thread loads component q of its line (r,
-  // or e0 and x' of both neighbour lines) into register slot sl and later stores
-  // it into the step's parity slot
-  constexpr int L = SweepTypes<TI>::kAhead;
-  double rr[L];
-  TC re[L], rm[L], rp[L];
-  auto load_vec = [&](bool has, int off, int sl) {
-    if (has) {
-      if constexpr (FIRST) {
-        rr[sl] = __ldcg(rb + off);
-      } else {
-        re[sl] = __ldcg(e0b + off);
-        rm[sl] = __ldcg(xmb + off);
-        rp[sl] = __ldcg(xpb + off);
+  // vector entries of step u in register slot sl: r, or e0 and x' of both neighbour lines
+  TC re[L][4], rm[L][4], rp[L][4];   // first sweep: r in re
+  auto load_vec = [&](int u, int off, int sl) {
+    if (u < nvec) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if constexpr (FIRST) {
+          re[sl][c] = TC(__ldcg(rb + c * comp + off));
+        } else {
+          re[sl][c] = __ldcg(e0b + c * comp + off);
+          rm[sl][c] = __ldcg(xmb + c * comp + off);
+          rp[sl][c] = __ldcg(xpb + c * comp + off);
+        }
       }
     }
   };
-  auto store_vec = [&](bool has, int par, int sl) {
-    if (has) {
-      if constexpr (FIRST) {
-        reinterpret_cast<double*>(sm.vec[h][par])[l * 4 + q] = rr[sl];
-      } else {
-        TC* v = reinterpret_cast<TC*>(sm.vec[h][par]) + l * 4 + q;
-        v[0] = re[sl];
-        v[kLanes * 4] = rm[sl];
-        v[2 * kLanes * 4] = rp[sl];
-      }
-    }
-  };
-
-  // waits for stage t of the half; a wait that runs out is remembered and
-  // OR-reduced over the half by the step's barrier
-  bool wfail = false;
-  auto wait_full = [&](int t) {
-    if (!mbar_wait(&sm.full[h][t % S], (t / S) & 1)) wfail = true;
-  };
-  // this warp is done with stage t % S
-  auto release = [&](int t) {
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&sm.empty[h][t % S]);
-  };
-  // e of step t from the forward blocks of stage s and the step's vector entries;
-  // the first sweep also keeps e (row offset off) for the later sweeps
-  auto rhs = [&](int t, int s, int off) -> TC {
+  // e of a step from stage s and the step's vector entries (first sweep: va = r;
+  // later sweeps: va = e0, vm = x'[i-1], vp = x'[i+1]); the first sweep also
+  // keeps e (row offset off)
+  auto rhs = [&](int s, int off, const TC (&va)[4], const TC (&vm)[4], const TC (&vp)[4], TC (&e)[4]) {
     const unsigned char* m = sm.mat[h][s];
-    const unsigned char* vsb = sm.vec[h][t & 1];
-    TC e;
     if constexpr (FIRST) {
-      TC iv[4], rvv[4];
-      load4(reinterpret_cast<const TI*>(m) + eo, iv);
-      load4(reinterpret_cast<const double*>(vsb) + l * 4, rvv);
-      e = iv[0] * rvv[0];
 #pragma unroll
-      for (int c = 1; c < 4; ++c) e += iv[c] * rvv[c];
-      if (a.e0 != nullptr && owner) reinterpret_cast<TC*>(a.e0)[vq + i + off] = e;
-    } else {
-      const TC* vs = reinterpret_cast<const TC*>(vsb);
-      TC pv[4], qv[4], xm[4], xp[4];
-      load4(reinterpret_cast<const TF*>(m) + eo, pv);
-      load4(reinterpret_cast<const TF*>(m + kBytesF) + eo, qv);
-      load4(vs + kLanes * 4 + l * 4, xm);
-      load4(vs + 2 * kLanes * 4 + l * 4, xp);
-      TC s1 = pv[0] * xm[0];
-      TC s2 = qv[0] * xp[0];
+      for (int r = 0; r < 4; ++r) {
+        TC iv[4];
+        load4(reinterpret_cast<const TI*>(m) + eo + r * kLanes * 4, iv);
+        e[r] = iv[0] * va[0];
 #pragma unroll
-      for (int c = 1; c < 4; ++c) {
-        s1 += pv[c] * xm[c];
-        s2 += qv[c] * xp[c];
+        for (int c = 1; c < 4; ++c) e[r] += iv[c] * va[c];
       }
-      e = vs[l * 4 + q] + s1 - s2;
+      if (a.e0 != nullptr && owner) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) e0w[r * comp + off] = e[r];
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        TC pv[4], qv[4];
+        load4(reinterpret_cast<const TF*>(m) + eo + r * kLanes * 4, pv);
+        load4(reinterpret_cast<const TF*>(m + kBytesF) + eo + r * kLanes * 4, qv);
+        TC s1 = pv[0] * vm[0];
+        TC s2 = qv[0] * vp[0];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) {
+          s1 += pv[c] * vm[c];
+          s2 += qv[c] * vp[c];
+        }
+        e[r] = va[r] + s1 - s2;
+      }
     }
-    return e;
+  };
+  // y += B x for the block at byte offset boff of stage s
+  auto addmv = [&](int s, uint32_t boff, const TC (&xv)[4], TC (&y)[4]) {
+    const TF* B = reinterpret_cast<const TF*>(sm.mat[h][s] + boff) + eo;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      TC bv[4];
+      load4(B + r * kLanes * 4, bv);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) y[r] += bv[c] * xv[c];
+    }
   };
 
-  // step 0's entries stored, steps 1 .. L in flight
-  int voff = rf0;   // row of the latest vector load
-  load_vec(0 < nvec, voff, 0);
-  store_vec(0 < nvec, 0, 0);
-#pragma unroll
-  for (int u = 1; u <= L; ++u) {
-    voff += rstep;
-    load_vec(u < nvec, voff, u % L);
-  }
-  half_sync(h);
+  bool fail = false;
+  int consumed = 0;   // steps of this half whose stage has been consumed
+  TC dprev[4] = {TC(0), TC(0), TC(0), TC(0)};   // d_{-1} = d'_{nc} = 0
 
-  int tstop = -1;     // step at which a wait ran out
+  // ---- forward elimination of this half (unrolled by L: register slots are static) ----
+  int voff = rf0;   // row of the latest vector load
+#pragma unroll
+  for (int u = 0; u < L; ++u) {
+    load_vec(u, voff, u);
+    voff += rstep;
+  }
   int roff = rf0;   // row of the current forward step
-  // ---- forward eliminations of both halves (unrolled by L: register slots are static) ----
 #pragma unroll 1
-  for (int tb = 0; tb < nf && tstop < 0; tb += L) {
+  for (int tb = 0; tb < nf && !fail; tb += L) {
 #pragma unroll
     for (int uu = 0; uu < L; ++uu) {
       const int t = tb + uu;
-      if (t < nf && tstop < 0) {
+      if (t < nf && !fail) {
         const int s = t % S;
-        wait_full(t);
-        const TC e = rhs(t, s, roff);
-        TC gv[4], dp[4];
-        load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
-        release(t);
-        load4(&sm.xchg[h][(t + 1) & 1][l][0], dp);
-        TC d = e;
+        if (!wait_full(t)) {
+          fail = true;
+        } else {
+          TC d[4];
+          rhs(s, roff, re[uu], rm[uu], rp[uu], d);
+          addmv(s, kOffG, dprev, d);
+          consumed = t + 1;
+          advance(t);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) d += gv[c] * dp[c];
-        sm.xchg[h][t & 1][l][q] = d;
-        if (owner) dvb[roff] = d;
-        roff += rstep;
-        store_vec(t + 1 < nvec, (t + 1) & 1, (uu + 1) % L);   // step t+1's entries, published by the barrier
-        voff += rstep;
-        load_vec(t + 1 + L < nvec, voff, (uu + 1) % L);       // and the slot refilled L steps ahead
-        if (half_sync_or(h, wfail)) tstop = t;
-      }
-    }
-  }
-  if (tstop >= 0 && l == 0 && q == 0) sm.failed[h] = 1;
-  consumers_sync();   // (A) both forward eliminations done
-  // ---- twist row k (wall half) ----
-  if (!(sm.failed[0] || sm.failed[1]) && h == 0) {
-    const int t = k;
-    const int s = t % S;
-    const int koff = k * ni;
-    wait_full(t);
-    const TC e = rhs(t, s, koff);
-    TC gv[4], hv[4], dm[4], dpl[4];
-    load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffG) + eo, gv);
-    load4(reinterpret_cast<const TF*>(sm.mat[h][s] + kOffH) + eo, hv);
-    release(t);
-    load4(&sm.xchg[0][(k + 1) & 1][l][0], dm);                        // d_{k-1}
-    if (nf1 > 0) load4(&sm.xchg[1][(nf1 + 1) & 1][l][0], dpl);        // d'_{k+1}
-    else dpl[0] = dpl[1] = dpl[2] = dpl[3] = TC(0);
-    TC xv = e;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) xv += gv[c] * dm[c];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) xv += hv[c] * dpl[c];
-    sm.xk[l][q] = xv;
-    if (owner) xb[koff] = TX(xv);
-    if (half_sync_or(h, wfail)) {
-      tstop = t;
-      if (l == 0 && q == 0) sm.failed[h] = 1;
-    }
-  }
-  consumers_sync();   // (B) x_k visible to both halves
-  // ---- back substitutions of both halves, outward from the twist row ----
-  const int t0 = h == 0 ? k + 1 : nf;
-  if (!(sm.failed[0] || sm.failed[1])) {
-    const int bstep = -rstep;                               // outward from the twist row
-    int boff = (h == 0 ? k - 1 : k + 1) * ni;               // row of back step t0
-    int poff = boff;                                        // row of the next prefetch
-    TC dbuf[kBackAhead];
-#pragma unroll
-    for (int u = 0; u < kBackAhead; ++u) {
-      dbuf[u] = t0 + u < nsteps ? dvb[poff] : TC(0);
-      poff += bstep;
-    }
-#pragma unroll 1
-    for (int b0 = t0; b0 < nsteps && tstop < 0; b0 += kBackAhead) {
-#pragma unroll
-      for (int u = 0; u < kBackAhead; ++u) {
-        const int t = b0 + u;
-        if (t < nsteps && tstop < 0) {
-          const int s = t % S;
-          wait_full(t);
-          TC cv[4], xn[4];
-          load4(reinterpret_cast<const TF*>(sm.mat[h][s]) + eo, cv);
-          release(t);
-          load4(t == t0 ? &sm.xk[l][0] : &sm.xchg[h][(t + 1) & 1][l][0], xn);
-          TC acc = cv[0] * xn[0];
-#pragma unroll
-          for (int c = 1; c < 4; ++c) acc += cv[c] * xn[c];
-          const TC xv = dbuf[u] - acc;
-          sm.xchg[h][t & 1][l][q] = xv;
-          if (owner) xb[boff] = TX(xv);
-          boff += bstep;
-          if (t + kBackAhead < nsteps) dbuf[u] = dvb[poff];
-          poff += bstep;
-          if (half_sync_or(h, wfail)) tstop = t;
+          for (int r = 0; r < 4; ++r) {
+            if (owner) dvb[r * comp + roff] = d[r];
+            dprev[r] = d[r];
+          }
+          roff += rstep;
+          load_vec(t + L, voff, uu);   // refill the slot L steps ahead
+          voff += rstep;
         }
       }
     }
   }
-  if (tstop >= 0 && l == 0 && q == 0) {
-    // a copy never landed: record it, and give the copies that may still be in
-    // flight for this half (issued for steps tstop .. tstop+S-1) a bounded time
-    if (a.err != nullptr) atomicExch(a.err, 1u);
+  // (A): the far-field half's d'_{k+1} to the wall half
+  if (h == 1) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) sm.dk[l][r] = dprev[r];
+  }
+  if (fail && l == 0) sm.failed[h] = 1;
+  halves_sync();
+  // ---- twist row k (wall half): its vector entries are in slot k % L ----
+  if (h == 0 && !(sm.failed[0] || sm.failed[1])) {
+    const int t = k;
+    const int s = t % S;
+    if (!wait_full(t)) {
+      fail = true;
+    } else {
+      TC xv[4], dpl[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) dpl[r] = sm.dk[l][r];
+      // the twist's vector entries from register slot k % L, by conditional moves
+      // over the static slots (a runtime slot index would put the slots in memory)
+      TC ve[4], vm[4], vp[4];
+      auto take = [&](auto slot) {
+        constexpr int sl = decltype(slot)::value;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          ve[c] = re[sl][c];
+          vm[c] = rm[sl][c];
+          vp[c] = rp[sl][c];
+        }
+      };
+      switch (k % L) {
+        case 0: take(std::integral_constant<int, 0>{}); break;
+        case 1: if constexpr (L > 1) take(std::integral_constant<int, (L > 1 ? 1 : 0)>{}); break;
+        case 2: if constexpr (L > 2) take(std::integral_constant<int, (L > 2 ? 2 : 0)>{}); break;
+        default: if constexpr (L > 3) take(std::integral_constant<int, (L > 3 ? 3 : 0)>{}); break;
+      }
+      rhs(s, k * ni, ve, vm, vp, xv);
+      addmv(s, kOffG, dprev, xv);
+      addmv(s, kOffH, dpl, xv);
+      consumed = t + 1;
+      advance(t);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        sm.xk[l][r] = xv[r];
+        if (owner) xb[r * comp + k * ni] = TX(xv[r]);
+      }
+    }
+    if (fail && l == 0) sm.failed[0] = 1;
+  }
+  halves_sync();   // (B) x_k visible to both halves
+  // ---- back substitution of this half, outward from the twist row ----
+  if (!(sm.failed[0] || sm.failed[1])) {
+    const int t0 = h == 0 ? k + 1 : nf;
+    const int bstep = -rstep;
+    int boff = (h == 0 ? k - 1 : k + 1) * ni;   // row of back step t0
+    int poff = boff;                           // row of the next prefetch
+    TC xn[4], dbuf[LB][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) xn[r] = sm.xk[l][r];
+#pragma unroll
+    for (int u = 0; u < LB; ++u) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) dbuf[u][r] = t0 + u < nsteps ? dvb[r * comp + poff] : TC(0);
+      poff += bstep;
+    }
 #pragma unroll 1
-    for (int u = tstop; u < tstop + S && u < nsteps; ++u) (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
+    for (int b0 = t0; b0 < nsteps && !fail; b0 += LB) {
+#pragma unroll
+      for (int u = 0; u < LB; ++u) {
+        const int t = b0 + u;
+        if (t < nsteps && !fail) {
+          const int s = t % S;
+          if (!wait_full(t)) {
+            fail = true;
+          } else {
+            const TF* Cb = reinterpret_cast<const TF*>(sm.mat[h][s]) + eo;
+            TC xv[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              TC cv[4];
+              load4(Cb + r * kLanes * 4, cv);
+              TC acc = cv[0] * xn[0];
+#pragma unroll
+              for (int c = 1; c < 4; ++c) acc += cv[c] * xn[c];
+              xv[r] = dbuf[u][r] - acc;
+            }
+            consumed = t + 1;
+            advance(t);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              if (owner) xb[r * comp + boff] = TX(xv[r]);
+              xn[r] = xv[r];
+              if (t + LB < nsteps) dbuf[u][r] = dvb[r * comp + poff];
+            }
+            boff += bstep;
+            poff += bstep;
+          }
+        }
+      }
+    }
+  }
+  if (fail || sm.failed[0] || sm.failed[1]) {
+    // a copy never landed (here or in the other half): record it, and give the
+    // copies this warp issued and has not consumed a bounded time to land
+    // before the CTA's shared memory goes away
+    if (l == 0) {
+      if (a.err != nullptr) atomicExch(a.err, 1u);
+#pragma unroll 1
+      for (int u = consumed; u < issued; ++u) (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
+    }
   }
 }
 
 template <typename TI, bool FIRST>
-void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s) {
+void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s, int variant) {
   if (b.ngroups == 0) return;
+  if (variant == kSweepRows) {
+    launch_sweep_rows<TI, FIRST>(b, a, last, s);
+    return;
+  }
   if (last) k_sweep<TI, FIRST, true><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TI>), s>>>(b, a);
   else k_sweep<TI, FIRST, false><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TI>), s>>>(b, a);
 }
 
 cudaError_t sweep_init() {
-  cudaError_t e = cudaSuccess;
+  cudaError_t e = sweep_rows_init();
   auto set = [&](const void* f, size_t bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   };
@@ -489,9 +453,9 @@ cudaError_t sweep_init() {
   return e;
 }
 
-template void launch_sweep<float, true>(const Batch&, const SweepArgs&, bool, cudaStream_t);
-template void launch_sweep<float, false>(const Batch&, const SweepArgs&, bool, cudaStream_t);
-template void launch_sweep<double, true>(const Batch&, const SweepArgs&, bool, cudaStream_t);
-template void launch_sweep<double, false>(const Batch&, const SweepArgs&, bool, cudaStream_t);
+template void launch_sweep<float, true>(const Batch&, const SweepArgs&, bool, cudaStream_t, int);
+template void launch_sweep<float, false>(const Batch&, const SweepArgs&, bool, cudaStream_t, int);
+template void launch_sweep<double, true>(const Batch&, const SweepArgs&, bool, cudaStream_t, int);
+template void launch_sweep<double, false>(const Batch&, const SweepArgs&, bool, cudaStream_t, int);
 
 }  // namespace a2d

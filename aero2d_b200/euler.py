@@ -99,8 +99,10 @@ def van_albada(a, b, eps):
 
 
 def _precision_of(dtype) -> int:
-    """float64 -> all-FP64 path; float32 -> mixed precision (FP32 linearisation
-    and Krylov basis around an FP64 residual, factorisation and update)."""
+    """float64 -> all-FP64 path; float32 -> mixed precision for the implicit
+    solver (FP32 linearisation and Krylov basis around an FP64 residual,
+    factorisation and update) and the FP32 explicit iteration (residual, local
+    time steps, smoothing and stage update in FP32)."""
     name = getattr(dtype, "__name__", None) or str(dtype)
     try:
         name = np.dtype(dtype).name

@@ -69,9 +69,16 @@ class DeviceGrid:
 
 
 class Plan:
-    """A batch of cases bound to one device workspace (include/aero2d_b200.h)."""
+    """A batch of cases bound to one device workspace (include/aero2d_b200.h).
 
-    def __init__(self, grids: list[DeviceGrid], winf: np.ndarray, params: _lib.Params, device=None):
+    `tuning`: the launch configuration (aero2d_b200.autotune): "cached" (the
+    default) applies the autotuner's stored choice for this plan's grid sizes
+    and precision if there is one; "auto" also measures and stores it when there
+    is none; None keeps the library's defaults; a (jvp_tile, sweep) pair sets it.
+    Results do not depend on it."""
+
+    def __init__(self, grids: list[DeviceGrid], winf: np.ndarray, params: _lib.Params, device=None,
+                 tuning="cached"):
         lib = _lib.load()
         self.lib = lib
         self.device = device_of(device if device is not None else grids[0].device)
@@ -92,6 +99,30 @@ class Plan:
         with torch.cuda.device(self.device):
             _lib.check(lib.a2d_plan_bind(h, _ptr(self.workspace), n.value, self.stream))
         self.total_ni = sum(g.ni for g in grids)
+        if tuning is not None:
+            from . import autotune
+            if isinstance(tuning, str):
+                autotune.apply(self, measure=(tuning == "auto"))
+            else:
+                self.set_tuning(*tuning)
+
+    @property
+    def shapes(self) -> list[tuple[int, int]]:
+        return [(g.ni, g.nc) for g in self.grids]
+
+    def set_tuning(self, jvp_tile: str = "32x8", sweep: str = "lanes") -> None:
+        """The launch configuration: the FP32 JVP's tile shape and the line
+        sweep's kernel variant (include/aero2d_b200.h, A2D_JVP_TILE_*, A2D_SWEEP_*)."""
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.a2d_plan_set_tuning(self.handle, _lib.JVP_TILES[jvp_tile],
+                                                    _lib.SWEEP_VARIANTS[sweep], self.stream))
+
+    def tuning(self) -> tuple[str, str]:
+        t, v = C.c_int(), C.c_int()
+        _lib.check(self.lib.a2d_plan_get_tuning(self.handle, C.byref(t), C.byref(v)))
+        inv_t = {b: a for a, b in _lib.JVP_TILES.items()}
+        inv_v = {b: a for a, b in _lib.SWEEP_VARIANTS.items()}
+        return inv_t[t.value], inv_v[v.value]
 
     @property
     def stream(self) -> int:

@@ -18,7 +18,7 @@ device workspace.
     svc = EulerService(classes=[(g128, 16), (g256, 16)])     # ragged slots
     rid = svc.submit(0.5, np.arange(-4, 17, 1.0), grid=dg)   # dg: that request's grid
     done = svc.run()                 # or svc.step() in your own loop + svc.poll()
-    res = svc.result(rid)            # dict: alpha, cl, cd, cm, cp, converged, nsteps
+    res = svc.result(rid)            # dict: alpha, cl, cd, cm, cp, converged, nsteps, drop
 """
 from __future__ import annotations
 
@@ -75,9 +75,11 @@ class EulerService:
     def __init__(self, grid: OGrid | DeviceGrid | None = None, slots: int = 64, dtype=np.float32, device=None,
                  tol: float = 1e-8, max_iter: int = 200, gmres_restart: int = 30, cfl0: float = 10.0,
                  cfl_max: float = 300.0, gmres_tol: float = 0.01, jacobi_sweeps: int = 4,
-                 max_update: float = 0.2, classes: Optional[Sequence[tuple]] = None):
+                 max_update: float = 0.2, classes: Optional[Sequence[tuple]] = None, tuning="cached"):
         """`grid` + `slots` for one grid size, or `classes` = [(grid, slots), ...]
-        with one grid per size (the class's default grid)."""
+        with one grid per size (the class's default grid).  `tuning` as for
+        plan.Plan: "cached", "auto" (measured on the idle slots at creation on a
+        cache miss), None, or a (jvp_tile, sweep) pair."""
         if classes is None:
             if grid is None:
                 raise ValueError("give a grid (and slots) or classes")
@@ -112,6 +114,26 @@ class EulerService:
         with torch.cuda.device(self.device):
             _lib.check(self.lib.a2d_service_bind(h, _ptr(self.workspace), n.value, self.stream))
         self._meta: dict[int, tuple] = {}
+        self._params = p
+        if tuning is not None:
+            self._tune(tuning)
+
+    def _tune(self, tuning) -> None:
+        """Applies (or, with "auto" on a cache miss, measures) the launch
+        configuration on the service's own plan while every slot is idle, then
+        retires every slot again."""
+        from . import autotune
+        view = _PlanView(self)
+        if isinstance(tuning, str):
+            measured = tuning == "auto" and autotune.TuningCache().get(autotune.plan_key(view)) is None
+            autotune.apply(view, measure=(tuning == "auto"))
+            if measured:
+                view.retire_all()
+        else:
+            view.set_tuning(*tuning)
+
+    def tuning(self) -> tuple[str, str]:
+        return _PlanView(self).tuning()
 
     @property
     def stream(self) -> int:
@@ -166,6 +188,12 @@ class EulerService:
         _lib.check(self.lib.a2d_service_pending(self.handle, C.byref(q), C.byref(r)))
         return q.value, r.value
 
+    def stats(self) -> tuple[int, int]:
+        """(kernel launches of one Newton step, Newton steps taken since bind)."""
+        k, n = C.c_int(), C.c_longlong()
+        _lib.check(self.lib.a2d_service_stats(self.handle, C.byref(k), C.byref(n)))
+        return k.value, n.value
+
     def result(self, rid: int) -> dict:
         """A finished request's per-point results; releases the request (and its grid)."""
         mach, alphas, dg = self._meta[rid]
@@ -174,6 +202,9 @@ class EulerService:
         cp = np.empty((n, dg.ni))
         conv = np.empty(n, np.int32)
         steps = np.empty(n, np.int32)
+        drop = np.empty(n)
+        _lib.check(self.lib.a2d_service_result_drop(self.handle, C.c_longlong(rid),
+                                                    drop.ctypes.data_as(C.POINTER(C.c_double))))
         _lib.check(self.lib.a2d_service_result(self.handle, C.c_longlong(rid),
                                                coef.ctypes.data_as(C.POINTER(C.c_double)),
                                                cp.ctypes.data_as(C.POINTER(C.c_double)),
@@ -181,7 +212,7 @@ class EulerService:
                                                steps.ctypes.data_as(C.POINTER(C.c_int))))
         del self._meta[rid]
         return {"mach": mach, "alpha": alphas, "cl": coef[:, 0], "cd": coef[:, 1], "cm": coef[:, 2], "cp": cp,
-                "converged": conv.astype(bool), "nsteps": steps}
+                "converged": conv.astype(bool), "nsteps": steps, "drop": drop}
 
     def run(self, max_steps: Optional[int] = None) -> list[int]:
         """Steps until the queue and every slot are empty (or max_steps steps);
@@ -197,3 +228,36 @@ class EulerService:
             if max_steps is not None and k >= max_steps:
                 break
         return done
+
+
+class _PlanView:
+    """The service's own plan, seen as a plan.Plan by the autotuner."""
+
+    def __init__(self, svc: "EulerService"):
+        h = C.c_void_p()
+        _lib.check(svc.lib.a2d_service_plan(svc.handle, C.byref(h)))
+        self.handle, self.lib, self.device, self.params = h, svc.lib, svc.device, svc._params
+        self.shapes = [(dg.ni, dg.nc) for dg, n in svc.classes for _ in range(n)]
+
+    def _call(self, name, *args):
+        with torch.cuda.device(self.device):
+            _lib.check(getattr(self.lib, name)(self.handle, *args, stream_handle(self.device)))
+
+    def set_tuning(self, jvp_tile: str = "32x8", sweep: str = "lanes") -> None:
+        self._call("a2d_plan_set_tuning", _lib.JVP_TILES[jvp_tile], _lib.SWEEP_VARIANTS[sweep])
+
+    def tuning(self) -> tuple[str, str]:
+        t, v = C.c_int(), C.c_int()
+        _lib.check(self.lib.a2d_plan_get_tuning(self.handle, C.byref(t), C.byref(v)))
+        return ({b: a for a, b in _lib.JVP_TILES.items()}[t.value],
+                {b: a for a, b in _lib.SWEEP_VARIANTS.items()}[v.value])
+
+    def init_freestream(self) -> None:
+        self._call("a2d_init_freestream")
+
+    def newton_step(self) -> None:
+        self._call("a2d_newton_step")
+
+    def retire_all(self) -> None:
+        n = len(self.shapes)
+        self._call("a2d_case_retire", n, (C.c_int * n)(*range(n)))

@@ -99,6 +99,19 @@ int a2d_plan_bind(a2d_plan* plan, void* workspace, size_t bytes, void* stream);
 int a2d_plan_destroy(a2d_plan* plan);
 int a2d_plan_ncases(const a2d_plan* plan);
 
+/* ---- launch-configuration knobs, chosen per (grid sizes, precision) by the autotuner
+ * (aero2d_b200.autotune); no counterpart in the reference.  Results do not depend on
+ * them: every variant computes the same arithmetic in the same order. ---- */
+#define A2D_JVP_TILE_32x8 0     /* tile shape (i x j cells) of the FP32 JVP stencil; FP64 plans */
+#define A2D_JVP_TILE_32x16 1    /* always use 32 x 8 */
+#define A2D_JVP_TILE_64x4 2
+#define A2D_JVP_TILE_16x16 3
+#define A2D_SWEEP_LANES 0       /* line sweep: one warp per half line group, a lane per line   */
+#define A2D_SWEEP_ROWS 1        /* line sweep: four warps per half line group, a warp per block row */
+/* any time, bound or not; a change re-captures the Newton step's graph at the next step */
+int a2d_plan_set_tuning(a2d_plan* plan, int jvp_tile, int sweep_variant, void* stream);
+int a2d_plan_get_tuning(const a2d_plan* plan, int* jvp_tile, int* sweep_variant);
+
 /* vector I/O in the reference layout [4][ni][nc] of one case (device pointers) */
 int a2d_vec_set(a2d_plan* plan, int slot, int case_index, const double* src, void* stream);
 int a2d_vec_get(const a2d_plan* plan, int slot, int case_index, double* dst, void* stream);
@@ -196,7 +209,19 @@ int a2d_service_poll(a2d_service* service, long long* ids, int max_ids, int* n);
 /* a finished request's results to host arrays: coef [npoints][3], cp [npoints][ni] or NULL,
  * converged [npoints], nsteps [npoints]; releases the request */
 int a2d_service_result(a2d_service* service, long long id, double* coef, double* cp, int* converged, int* nsteps);
+/* a finished request's per-point residual drop (last finite residual norm / r0) to a host
+ * array [npoints]: a point reached params.tol when its drop is below it (the reference's own
+ * converged flag above asks only three orders, aero2d/implicit.py:252); call before
+ * a2d_service_result, which releases the request */
+int a2d_service_result_drop(a2d_service* service, long long id, double* drop);
 int a2d_service_pending(a2d_service* service, int* queued, int* running);
+/* the service's own plan (borrowed; it lives as long as the service): its slots in class
+ * order, for a2d_plan_set_tuning and the measurement calls.  Stepping it directly, outside
+ * a2d_service_step, is only safe while no request is queued or running */
+int a2d_service_plan(a2d_service* service, a2d_plan** plan);
+/* kernel launches of one Newton step of the service's plan (counted in its captured graph; 0
+ * before the first step) and the Newton steps the service has taken since bind */
+int a2d_service_stats(a2d_service* service, int* kernels_per_step, long long* newton_steps);
 int a2d_service_destroy(a2d_service* service);
 /* per-step histories to host arrays [steps][ncases] (residual norm, Cl); steps <= max_iter */
 int a2d_history(const a2d_plan* plan, int steps, double* rn, double* cl, void* stream);

@@ -107,6 +107,25 @@ def test_explicit_rk_vs_oracle(cuda):
     assert abs(rg.cl[0] - ro["cl"][0]) < 1e-10
 
 
+def test_explicit_rk_fp32_vs_oracle(cuda):
+    """dtype=float32: the explicit RK4 + IRS iteration runs in FP32 (residual,
+    local time steps, smoothing and stage update, as the reference casts its
+    explicit path to the solver dtype, aero2d/euler.py:222-234).  Against the
+    FP64 oracle: FP32 rounding, not the FP64 path, and the state holds FP32
+    values."""
+    g = grid("0012", 33, 25)
+    om = EulerModel(g.x, g.y)
+    ro = om.solve([0.5], [2.0], n_iter=6, chunk=3, tol=0.0)
+    s = EulerSolver(g, dtype=np.float32, device=cuda)
+    rg = s.solve([0.5], [2.0], n_iter=6, chunk=3, tol=0.0, verbose=False)
+    U = rg.U[0].cpu().numpy()
+    dU = ro["U"][0] - om.init_state(om.freestream(0.5, 2.0))
+    err = np.max(np.abs(U - ro["U"][0])) / np.max(np.abs(dU))
+    assert 1e-9 < err < 1e-4, err
+    assert abs(rg.cl[0] - ro["cl"][0]) < 1e-5
+    assert np.array_equal(U.astype(np.float32).astype(np.float64), U)
+
+
 def test_nan_case_is_isolated(cuda):
     """A case whose state is non-finite is rolled back, frozen after five
     failures and flagged non-converged; the other cases are unaffected."""

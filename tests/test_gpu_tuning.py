@@ -1,0 +1,55 @@
+"""The launch-configuration knobs on the GPU: every (JVP tile shape, sweep
+variant) takes bitwise the same Newton step, in FP64 and mixed precision, on a
+ragged batch (two grid sizes); the autotuner measures, stores and re-applies a
+choice through its cache."""
+import numpy as np
+import pytest
+import torch
+
+from aero2d_b200 import _lib, autotune
+from aero2d_b200.euler import EulerSolver
+from aero2d_b200.implicit import ImplicitEuler
+from aero2d_b200.plan import Plan
+from tests.helpers import grid
+
+pytestmark = pytest.mark.gpu
+
+
+def ragged_plan(dtype, cuda, tuning=None):
+    ga, gb = grid("2412", 65, 33), grid("0012", 49, 25)
+    sa, sb = EulerSolver(ga, dtype=dtype, device=cuda), EulerSolver(gb, dtype=dtype, device=cuda)
+    imp = ImplicitEuler(sa, gmres_restart=20)
+    machs, alphas = np.array([0.5, 0.7, 0.6]), np.array([2.0, 1.0, -1.0])
+    return Plan([sa.dgrid, sb.dgrid, sa.dgrid], sa.freestream(machs, alphas), imp.params(1e-10, 20), cuda,
+                tuning=tuning)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_every_configuration_takes_the_same_step(cuda, dtype):
+    pl = ragged_plan(dtype, cuda)
+    ref = None
+    for t, v in autotune.candidates(_lib.A2D_MIXED if dtype == np.float32 else _lib.A2D_FP64):
+        pl.set_tuning(t, v)
+        assert pl.tuning() == (t, v)
+        pl.init_freestream()
+        for _ in range(3):
+            pl.newton_step()
+        U = pl.get_batch(_lib.VEC_U)
+        sc = pl.scalars()
+        if ref is None:
+            ref = (U, sc)
+        else:
+            assert torch.equal(U, ref[0]), (t, v)
+            assert np.array_equal(sc, ref[1]), (t, v)
+
+
+def test_autotuner_measures_stores_and_reapplies(cuda, tmp_path, monkeypatch):
+    monkeypatch.setenv("AERO2D_B200_TUNING", str(tmp_path / "tuning.json"))
+    pl = ragged_plan(np.float32, cuda, tuning="auto")
+    cache = autotune.TuningCache()
+    key = autotune.plan_key(pl)
+    choice = cache.get(key)
+    assert choice is not None and pl.tuning() == choice
+    assert len(cache.load()[key]["ms"]) == len(autotune.candidates(_lib.A2D_MIXED))
+    pl2 = ragged_plan(np.float32, cuda, tuning="cached")
+    assert pl2.tuning() == choice
