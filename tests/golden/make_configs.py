@@ -3,7 +3,9 @@ the benchmark configurations, the known answers that the GPU parity tests and
 the bench's accuracy report compare against.  Run by hand in the build
 container (CPU only, about an hour on 8 cores; one spawned process per case):
 
-    python tests/golden/make_configs.py [--procs 8] [--only c1,c2,c3]
+    python tests/golden/make_configs.py [--procs 8] [--only c1,c2,c3] [--force]
+
+(cases already in the file are kept unless --force)
 
 Cases (all with the reference's ImplicitEuler defaults except GMRES restart 30,
 aero2d/implicit.py:68-70, from the uniform freestream, one case per solve):
@@ -101,13 +103,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--procs", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--only", default="c1,c2,c3")
+    ap.add_argument("--force", action="store_true", help="recompute cases already in the file")
     a = ap.parse_args()
     sys.path.insert(0, str(ROOT))
     only = set(a.only.split(","))
-    cases = case_list(only)
+    old = json.load(open(OUT)) if OUT.exists() else {"cases": {}}
+    cases = [c for c in case_list(only) if a.force or c["name"] not in old["cases"]]
     # longest cases first so the pool's tail is short
     cases.sort(key=lambda c: -c["grid"]["n_side"] * c["grid"]["nj"] * c["n_iter"])
-    old = json.load(open(OUT)) if OUT.exists() else {"cases": {}}
     with mp.get_context("spawn").Pool(a.procs) as pool:
         for res in pool.imap_unordered(solve_case, cases):
             old["cases"][res["name"]] = res
