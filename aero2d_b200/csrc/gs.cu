@@ -211,6 +211,8 @@ struct GsRing {
   const TB* V;        // first vector of the slice, at the chunk's first entry
   size_t vstride;
   const double* w;    // at the chunk's first entry
+  uint64_t pol;       // L2 policy of the basis runs: evict first, so that w (re-read by the
+                      // three passes of an Arnoldi step) stays in L2
 
   __device__ void init(unsigned char* smem, const GsArgs<TB>& a, const Chunk& ch, size_t base) {
     full = reinterpret_cast<uint64_t*>(smem);
@@ -224,6 +226,7 @@ struct GsRing {
     V = a.V + (size_t)a.q0 * a.vstride + base;
     vstride = a.vstride;
     w = a.w + base;
+    pol = l2_evict_first();
     if (threadIdx.x == 0) {
       for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
       mbar_init_fence();
@@ -243,7 +246,7 @@ struct GsRing {
     unsigned char* st = stages + (size_t)s * stage_bytes;
     mbar_arrive_expect(&full[s], (uint32_t)n * (uint32_t)(nq * sizeof(TB) + 8));
     for (int q = 0; q < nq; ++q)
-      bulk_load(st + (size_t)q * E * sizeof(TB), V + (size_t)q * vstride + e0, n * sizeof(TB), &full[s]);
+      bulk_load_hint(st + (size_t)q * E * sizeof(TB), V + (size_t)q * vstride + e0, n * sizeof(TB), &full[s], pol);
     bulk_load(st + (size_t)nq * E * sizeof(TB), w + e0, n * 8, &full[s]);
   }
   __device__ const TB* vec(int u, int q) const {

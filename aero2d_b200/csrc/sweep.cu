@@ -40,6 +40,7 @@
 // (products summed over the columns in order), so results are bitwise
 // repeatable.
 #include <type_traits>
+#include <utility>
 
 #include "batch.cuh"
 #include "kernels.cuh"
@@ -57,14 +58,14 @@ template <> struct SweepTypes<float> {
   using TF = __half;
   using TC = float;
   static constexpr int kStages = 6;     // bulk-copy ring stages per half
-  static constexpr int kAhead = 4;      // steps between loading a vector entry and its use
+  static constexpr int kAhead = 8;      // steps between loading a vector entry and its use
   static constexpr int kBackAhead = 8;  // register prefetch depth of d in the back substitution
 };
 template <> struct SweepTypes<double> {
   using TF = double;
   using TC = double;
   static constexpr int kStages = 2;
-  static constexpr int kAhead = 2;
+  static constexpr int kAhead = 4;
   static constexpr int kBackAhead = 4;
 };
 
@@ -101,6 +102,14 @@ __device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
   v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
 }
 
+// f(integral_constant<int, sl>) for the runtime slot sl in [0, L): register
+// arrays indexed through it keep static indices (a runtime index would put them
+// in local memory)
+template <typename F, int... I>
+__device__ __forceinline__ void slot_dispatch(int sl, F&& f, std::integer_sequence<int, I...>) {
+  ((sl == I ? f(std::integral_constant<int, I>{}) : void()), ...);
+}
+
 // the 64 threads of the CTA (named barrier 1)
 __device__ __forceinline__ void halves_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kSweepThreads) : "memory"); }
 
@@ -119,8 +128,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   constexpr uint32_t kBytesI = SM::kBytesI, kBytesF = SM::kBytesF;
   constexpr uint32_t kOffG = FIRST ? kBytesI : 2 * kBytesF;   // G's block in a forward stage
   constexpr uint32_t kOffH = kOffG + kBytesF;                // H's block in the twist stage
-  constexpr int L = SweepTypes<TI>::kAhead;   // at most 4 (the twist's slot switch below)
-  static_assert(L >= 1 && L <= 4, "kAhead must be in [1, 4]");
+  constexpr int L = SweepTypes<TI>::kAhead;
   constexpr int LB = SweepTypes<TI>::kBackAhead;
 
   const Group grp = b.groups[blockIdx.x];
@@ -153,6 +161,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   const TI* INV = static_cast<const TI*>(a.INV);
   const TF* PQG = static_cast<const TF*>(a.PQG);
   const TF* CF = static_cast<const TF*>(a.CF);
+  const uint64_t pol = l2_evict_first();   // factor blocks are read once per sweep
   int issued = 0;
   auto issue = [&](int t) {
     const int j = row_of(t);
@@ -164,17 +173,17 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
     if (fwd) {
       if constexpr (FIRST) {
         mbar_arrive_expect(bar, kBytesI + (twist ? 2 : 1) * kBytesF);
-        bulk_load(m, INV + o, kBytesI, bar);
-        bulk_load(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, bar);
-        if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
+        bulk_load_hint(m, INV + o, kBytesI, bar, pol);
+        bulk_load_hint(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, bar, pol);
+        if (twist) bulk_load_hint(m + kOffH, CF + o, kBytesF, bar, pol);
       } else {
         mbar_arrive_expect(bar, (twist ? 4 : 3) * kBytesF);
-        bulk_load(m, PQG + 3 * o, 3 * kBytesF, bar);   // P, Q, G: one run
-        if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
+        bulk_load_hint(m, PQG + 3 * o, 3 * kBytesF, bar, pol);   // P, Q, G: one run
+        if (twist) bulk_load_hint(m + kOffH, CF + o, kBytesF, bar, pol);
       }
     } else {
       mbar_arrive_expect(bar, kBytesF);
-      bulk_load(m, CF + o, kBytesF, bar);
+      bulk_load_hint(m, CF + o, kBytesF, bar, pol);
     }
   };
   if (l == 0)
@@ -202,8 +211,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   const size_t comp = (size_t)nc * ni;         // stride between the components of a case vector
   // per-line bases: row offsets within a component plane stay 32-bit
   const TC* e0b = reinterpret_cast<const TC*>(a.e0) + vbase + i;
+  const TC* xcb = reinterpret_cast<const TC*>(a.xprev) + vbase + i;
   const TC* xmb = reinterpret_cast<const TC*>(a.xprev) + vbase + im;
   const TC* xpb = reinterpret_cast<const TC*>(a.xprev) + vbase + ip;
+  // x' of the neighbour lines comes from the neighbour lanes by shuffles; the
+  // group's first lane and its last line's lane load the neighbour outside the group
+  const int lastl = grp.n - 1;
   const double* rb = a.r + vbase + i;
   TC* e0w = reinterpret_cast<TC*>(a.e0) + vbase + i;
   // d_j in the compute type: in x itself, or (last sweep, FP64 x) in the scratch
@@ -214,8 +227,10 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   const int rf0 = h == 0 ? 0 : (nc - 1) * ni;
   const int nvec = h == 0 ? k + 1 : nf1;       // steps with vector entries (forward, and the twist)
 
-  // vector entries of step u in register slot sl: r, or e0 and x' of both neighbour lines
-  TC re[L][4], rm[L][4], rp[L][4];   // first sweep: r in re
+  // vector entries of step u in register slot sl: r (first sweep) or e0, and x'
+  // of this line (rx), of the line before the group (rl, lane 0) and of the line
+  // after the group's last (rr, lane lastl)
+  TC re[L][4], rx[L][4], rl[L][4], rr[L][4];
   auto load_vec = [&](int u, int off, int sl) {
     if (u < nvec) {
 #pragma unroll
@@ -224,17 +239,29 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
           re[sl][c] = TC(__ldcg(rb + c * comp + off));
         } else {
           re[sl][c] = __ldcg(e0b + c * comp + off);
-          rm[sl][c] = __ldcg(xmb + c * comp + off);
-          rp[sl][c] = __ldcg(xpb + c * comp + off);
+          rx[sl][c] = __ldcg(xcb + c * comp + off);
+          if (l == 0) rl[sl][c] = __ldcg(xmb + c * comp + off);
+          if (l == lastl) rr[sl][c] = __ldcg(xpb + c * comp + off);
         }
       }
     }
   };
   // e of a step from stage s and the step's vector entries (first sweep: va = r;
-  // later sweeps: va = e0, vm = x'[i-1], vp = x'[i+1]); the first sweep also
-  // keeps e (row offset off)
-  auto rhs = [&](int s, int off, const TC (&va)[4], const TC (&vm)[4], const TC (&vp)[4], TC (&e)[4]) {
+  // later sweeps: va = e0, vx = x' of the line, vl / vr the outside neighbours);
+  // the first sweep also keeps e (row offset off).  All lanes call it (shuffles)
+  auto rhs = [&](int s, int off, const TC (&va)[4], const TC (&vx)[4], const TC (&vl)[4], const TC (&vr)[4],
+                 TC (&e)[4]) {
     const unsigned char* m = sm.mat[h][s];
+    TC vm[4], vp[4];   // x'[i-1], x'[i+1]
+    if constexpr (!FIRST) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const TC up = __shfl_up_sync(0xffffffffu, vx[c], 1);
+        const TC dn = __shfl_down_sync(0xffffffffu, vx[c], 1);
+        vm[c] = l == 0 ? vl[c] : up;
+        vp[c] = l == lastl ? vr[c] : dn;
+      }
+    }
     if constexpr (FIRST) {
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
@@ -300,7 +327,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
           fail = true;
         } else {
           TC d[4];
-          rhs(s, roff, re[uu], rm[uu], rp[uu], d);
+          rhs(s, roff, re[uu], rx[uu], rl[uu], rr[uu], d);
           addmv(s, kOffG, dprev, d);
           consumed = t + 1;
           advance(t);
@@ -333,25 +360,19 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
       TC xv[4], dpl[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) dpl[r] = sm.dk[l][r];
-      // the twist's vector entries from register slot k % L, by conditional moves
-      // over the static slots (a runtime slot index would put the slots in memory)
-      TC ve[4], vm[4], vp[4];
-      auto take = [&](auto slot) {
+      // the twist's vector entries from register slot k % L (static indices)
+      TC ve[4], vx[4], vl[4], vr[4];
+      slot_dispatch(k % L, [&](auto slot) {
         constexpr int sl = decltype(slot)::value;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           ve[c] = re[sl][c];
-          vm[c] = rm[sl][c];
-          vp[c] = rp[sl][c];
+          vx[c] = rx[sl][c];
+          vl[c] = rl[sl][c];
+          vr[c] = rr[sl][c];
         }
-      };
-      switch (k % L) {
-        case 0: take(std::integral_constant<int, 0>{}); break;
-        case 1: if constexpr (L > 1) take(std::integral_constant<int, (L > 1 ? 1 : 0)>{}); break;
-        case 2: if constexpr (L > 2) take(std::integral_constant<int, (L > 2 ? 2 : 0)>{}); break;
-        default: if constexpr (L > 3) take(std::integral_constant<int, (L > 3 ? 3 : 0)>{}); break;
-      }
-      rhs(s, k * ni, ve, vm, vp, xv);
+      }, std::make_integer_sequence<int, L>{});
+      rhs(s, k * ni, ve, vx, vl, vr, xv);
       addmv(s, kOffG, dprev, xv);
       addmv(s, kOffH, dpl, xv);
       consumed = t + 1;

@@ -172,6 +172,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     const TI* INV = static_cast<const TI*>(a.INV);
     const TF* PQG = static_cast<const TF*>(a.PQG);
     const TF* CF = static_cast<const TF*>(a.CF);
+    const uint64_t pol = l2_evict_first();   // factor blocks are read once per sweep
     int issued[2] = {0, 0};
     bool ok = true;
     const int smax = ns0 > ns1 ? ns0 : ns1;
@@ -195,17 +196,17 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
           if (fwd) {
             if constexpr (FIRST) {
               mbar_arrive_expect(bar, kBytesI + (twist ? 2 : 1) * kBytesF);
-              bulk_load(m, INV + o, kBytesI, bar);
-              bulk_load(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, bar);
-              if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
+              bulk_load_hint(m, INV + o, kBytesI, bar, pol);
+              bulk_load_hint(m + kBytesI, PQG + 3 * o + 2 * kBlockEntries, kBytesF, bar, pol);
+              if (twist) bulk_load_hint(m + kOffH, CF + o, kBytesF, bar, pol);
             } else {
               mbar_arrive_expect(bar, (twist ? 4 : 3) * kBytesF);
-              bulk_load(m, PQG + 3 * o, 3 * kBytesF, bar);   // P, Q, G: one run
-              if (twist) bulk_load(m + kOffH, CF + o, kBytesF, bar);
+              bulk_load_hint(m, PQG + 3 * o, 3 * kBytesF, bar, pol);   // P, Q, G: one run
+              if (twist) bulk_load_hint(m + kOffH, CF + o, kBytesF, bar, pol);
             }
           } else {
             mbar_arrive_expect(bar, kBytesF);
-            bulk_load(m, CF + o, kBytesF, bar);
+            bulk_load_hint(m, CF + o, kBytesF, bar, pol);
           }
         }
         issued[h] = t + 1;

@@ -966,7 +966,7 @@ def main():
     ap.add_argument("--c4-sample", type=int, default=16, help="cases stepped one plan at a time")
     ap.add_argument("--c4-steps", type=int, default=10, help="Newton steps timed per sampled case")
     ap.add_argument("--served-rate", type=float, default=50.0, help="request arrivals per second")
-    ap.add_argument("--served-window", type=float, default=4.0, help="seconds of arrivals (0 skips)")
+    ap.add_argument("--served-window", type=float, default=2.0, help="seconds of arrivals (0 skips)")
     ap.add_argument("--served-chains", type=int, default=3, help="continuation chains per alpha sweep")
     ap.add_argument("--served-hbm-gb", type=float, default=16.0, help="workspace budget of the service")
     ap.add_argument("--served-max-iter", type=int, default=100, help="Newton steps per point at most")

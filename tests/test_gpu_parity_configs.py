@@ -148,5 +148,9 @@ def test_mixed_converged_solutions_vs_oracle(cuda, name):
                 assert shift[-1] <= 2e-3, (c["name"], xs, c["shock_x"])
         compared += 1
     assert compared >= (1 if name == "c1" else 3), f"{name}: only {compared} cases compared"
+    if name == "c3":
+        # the stiffest configuration (384 x 96, first spacing 1e-3, CFL up to 300): no sweep
+        # factor left the FP16 range in the whole solve
+        assert r["saturations"] == 0, r["saturations"]
     print(f"{name}: {compared} cases, max |dCm| {max(dcm):.2e}, shock shifts {shift}, "
           f"FP16 factor saturations {r['saturations']}")
