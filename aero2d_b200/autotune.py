@@ -8,9 +8,10 @@ are bitwise the same; include/aero2d_b200.h, a2d_plan_set_tuning):
             stencil, run gmres_restart + 1 times per Newton step: "32x8",
             "32x16", "64x4" or "16x16" (the halo is recomputed per tile, so
             taller tiles compute less and hold more shared memory);
-  sweep     the line sweep's kernel: "lanes" (one warp per half line group, a
-            lane solving all four block rows of its line) or "rows" (four warps
-            per half line group, a warp per block row).
+  sweep     the line sweep's kernel, by warps per half line group: "lanes"
+            (one warp, a lane solving all four block rows of its line),
+            "pairs" (two warps, two lanes per line with two block rows each)
+            or "rows" (four warps, a warp per block row).
 
 The best configuration depends on the grid sizes in a batch, the batch size and
 the precision.  `apply(plan, measure=True)` looks the plan's key up in the
@@ -34,7 +35,7 @@ from pathlib import Path
 from typing import Callable, Iterable, Optional
 
 JVP_TILES = ("32x8", "32x16", "64x4", "16x16")
-SWEEPS = ("lanes", "rows")
+SWEEPS = ("lanes", "rows", "pairs")
 DEFAULT = ("32x8", "lanes")
 
 

@@ -119,10 +119,11 @@ void launch_face_jac(const Batch& b, const JacArgs& a, cudaStream_t s);
 template <typename TJ, typename TF>
 void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s);
 
-// kernel variants of the line-Jacobi sweep, a plan's tuning knob: one warp per
-// half line group, a lane solving all four block rows of its line (sweep.cu), or
-// four warps per half line group, a warp per block row (sweep_rows.cu)
-enum : int { kSweepLanes = 0, kSweepRows = 1, kNumSweepVariants = 2 };
+// kernel variants of the line-Jacobi sweep, a plan's tuning knob, by warps per
+// half line group: one, a lane solving all four block rows of its line
+// (sweep.cu); two, two lanes per line with two block rows each (sweep_pairs.cu);
+// four, a warp per block row (sweep_rows.cu)
+enum : int { kSweepLanes = 0, kSweepRows = 1, kSweepPairs = 2, kNumSweepVariants = 3 };
 
 // one line-Jacobi sweep; FIRST: the sweep without i-coupling; last: x is the
 // FP64 result (else an intermediate vector).  Both variants compute the same
@@ -131,9 +132,12 @@ template <typename TI, bool FIRST>
 void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s, int variant = kSweepLanes);
 template <typename TI, bool FIRST>
 void launch_sweep_rows(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s);
+template <typename TI, bool FIRST>
+void launch_sweep_pairs(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s);
 
 // raises the dynamic shared-memory limit of the sweep kernels (host, once per device)
 cudaError_t sweep_init();
 cudaError_t sweep_rows_init();
+cudaError_t sweep_pairs_init();
 
 }  // namespace a2d

@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
   // vector entries of step u in register slot sl: r (first sweep) or e0, and x'
   // of this line (rx), of the line before the group (rl, lane 0) and of the line
   // after the group's last (rr, lane lastl)
-  TC re[L][4], rx[L][4], rl[L][4], rr[L][4];
+  TC re[L][4], rx[L][4], rl[L][4] = {}, rr[L][4] = {};   // rl / rr: loaded by the edge lanes only
   auto load_vec = [&](int u, int off, int sl) {
     if (u < nvec) {
 #pragma unroll
@@ -456,12 +456,17 @@ void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s,
     launch_sweep_rows<TI, FIRST>(b, a, last, s);
     return;
   }
+  if (variant == kSweepPairs) {
+    launch_sweep_pairs<TI, FIRST>(b, a, last, s);
+    return;
+  }
   if (last) k_sweep<TI, FIRST, true><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TI>), s>>>(b, a);
   else k_sweep<TI, FIRST, false><<<b.ngroups, kSweepThreads, sizeof(SweepSmem<TI>), s>>>(b, a);
 }
 
 cudaError_t sweep_init() {
   cudaError_t e = sweep_rows_init();
+  if (e == cudaSuccess) e = sweep_pairs_init();
   auto set = [&](const void* f, size_t bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   };

@@ -133,12 +133,24 @@ class OracleBaseline:
         import multiprocessing as mp
         ctx = mp.get_context("spawn")
         self.conns, self.procs = [], []
-        for k in range(procs):
-            a, b = ctx.Pipe()
-            p = ctx.Process(target=_oracle_worker, args=(k % CASES, seed, b), daemon=True)
-            p.start()
-            self.conns.append(a)
-            self.procs.append(p)
+        # one BLAS thread per process: the children inherit the environment and
+        # read it when they import numpy, before the worker function runs
+        threads = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")
+        saved = {v: os.environ.get(v) for v in threads}
+        os.environ.update({v: "1" for v in threads})
+        try:
+            for k in range(procs):
+                a, b = ctx.Pipe()
+                p = ctx.Process(target=_oracle_worker, args=(k % CASES, seed, b), daemon=True)
+                p.start()
+                self.conns.append(a)
+                self.procs.append(p)
+        finally:
+            for v, old in saved.items():
+                if old is None:
+                    os.environ.pop(v, None)
+                else:
+                    os.environ[v] = old
         for c in self.conns:
             c.recv()
         fx = [v for k, v in oracle_fixtures().items() if k.startswith("c2_")]
@@ -968,7 +980,9 @@ def main():
     ap.add_argument("--served-rate", type=float, default=50.0, help="request arrivals per second")
     ap.add_argument("--served-window", type=float, default=2.0, help="seconds of arrivals (0 skips)")
     ap.add_argument("--served-chains", type=int, default=3, help="continuation chains per alpha sweep")
-    ap.add_argument("--served-hbm-gb", type=float, default=16.0, help="workspace budget of the service")
+    ap.add_argument("--served-hbm-gb", type=float, default=4.0,
+                    help="workspace budget of the service (slots beyond those that saturate the GPU only "
+                         "add latency)")
     ap.add_argument("--served-max-iter", type=int, default=100, help="Newton steps per point at most")
     ap.add_argument("--served-wall-cap", type=float, default=150.0, help="seconds before the stream is cut")
     ap.add_argument("--profile", type=int, default=0, metavar="STEPS",
