@@ -214,18 +214,26 @@ __device__ __forceinline__ void mul4_store(const double A[16], const double B[16
     }
 }
 
+// Two warps per 32-line group (a lane per line): the even warp eliminates from
+// the wall, the odd warp from the far field, in parallel; they meet at the twist
+// row through shared memory (one named barrier of the pair), which the wall warp
+// finishes.  The arithmetic of every row is the same as one thread running both
+// eliminations after each other.
 template <typename TJ, typename TF>
 __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
+  __shared__ double cfar[2][16][kLanes];   // per group of the CTA: c'_{k+1} of each line
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gid = blockIdx.x * 4 + warp;
-  if (gid >= b.ngroups) return;
+  const int pair = warp >> 1;              // group slot of the CTA
+  const int half = warp & 1;               // 0: from the wall, 1: from the far field
+  const int gid = blockIdx.x * 2 + pair;
+  if (gid >= b.ngroups) return;            // both warps of the pair leave together
   const Group grp = b.groups[gid];
   if (!case_live(b, grp.cs, a.need)) return;
-  if (lane >= grp.n) return;
+  const bool own = lane < grp.n;           // lanes past the group's last line only meet the barrier
   const CaseDev cs = b.cases[grp.cs];
   const GridDev& g = cs.g;
   const int ni = g.ni, nc = g.nc;
-  const int i = grp.i0 + lane;
+  const int i = grp.i0 + (own ? lane : grp.n - 1);
   const int ip = (i + 1 == ni) ? 0 : i + 1;
   const int gp = ip / kLanes, lp = ip % kLanes;
   const TJ* JIL = static_cast<const TJ*>(a.JIL);
@@ -331,16 +339,18 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   double cprev[16];
 #pragma unroll
   for (int e = 0; e < 16; ++e) cprev[e] = 0.0;
-  for (int j = 0; j < k; ++j) {
-    double D[16], A[16], inv[16], Gm[16], T1[16];
-    assemble(j, D);
-    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
-    mul_add(A, cprev, D, 1.0);
-    inv4(D, inv);
-    mul(inv, A, Gm, 1.0);
-    load_block(JJR, cs.rows_nc1, nc + 1, grp.g, j + 1, lane, T1);
-    mul(inv, T1, cprev, 1.0);
-    store_row(j, inv, Gm, cprev);
+  if (half == 0 && own) {
+    for (int j = 0; j < k; ++j) {
+      double D[16], A[16], inv[16], Gm[16], T1[16];
+      assemble(j, D);
+      load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
+      mul_add(A, cprev, D, 1.0);
+      inv4(D, inv);
+      mul(inv, A, Gm, 1.0);
+      load_block(JJR, cs.rows_nc1, nc + 1, grp.g, j + 1, lane, T1);
+      mul(inv, T1, cprev, 1.0);
+      store_row(j, inv, Gm, cprev);
+    }
   }
   // From the far field, rows nc-1 .. k+1: den'_j = D_j - U_j c'_{j+1},
   // c'_j = den'_j^-1 L_j, G'_j = -den'_j^-1 U_j; later d'_j = inv'_j r_j + G'_j d'_{j+1},
@@ -348,17 +358,30 @@ __global__ void __launch_bounds__(128) k_factor(Batch b, FactorArgs a) {
   double cnext[16];
 #pragma unroll
   for (int e = 0; e < 16; ++e) cnext[e] = 0.0;
-  for (int j = nc - 1; j > k; --j) {
-    double D[16], A[16], Um[16], inv[16], Gm[16];
-    assemble(j, D);
-    load_block(JJR, cs.rows_nc1, nc + 1, grp.g, j + 1, lane, Um);
-    mul_add(Um, cnext, D, -1.0);
-    inv4(D, inv);
-    mul(inv, Um, Gm, -1.0);
-    load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
-    mul(inv, A, cnext, -1.0);
-    store_row(j, inv, Gm, cnext);
+  if (half == 1) {
+    if (own) {
+      for (int j = nc - 1; j > k; --j) {
+        double D[16], A[16], Um[16], inv[16], Gm[16];
+        assemble(j, D);
+        load_block(JJR, cs.rows_nc1, nc + 1, grp.g, j + 1, lane, Um);
+        mul_add(Um, cnext, D, -1.0);
+        inv4(D, inv);
+        mul(inv, Um, Gm, -1.0);
+        load_block(JJL, cs.rows_nc1, nc + 1, grp.g, j, lane, A);
+        mul(inv, A, cnext, -1.0);
+        store_row(j, inv, Gm, cnext);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) cfar[pair][e][lane] = cnext[e];
   }
+  asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");   // the pair's two warps
+  if (half == 1 || !own) {
+    if (nsat != 0 && a.sat != nullptr) atomicAdd(a.sat, (unsigned long long)nsat);
+    return;
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) cnext[e] = cfar[pair][e][lane];
   // Row k: den_k = D_k - L_k c_{k-1} - U_k c'_{k+1};
   // x_k = inv_k r_k + G_k d_{k-1} + H_k d'_{k+1}, G_k = -inv_k L_k, H_k = -inv_k U_k
   // (H is kept in the C slot of row k, which has no back substitution).
@@ -385,7 +408,7 @@ void launch_face_jac(const Batch& b, const JacArgs& a, cudaStream_t s) {
 template <typename TJ, typename TF>
 void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s) {
   if (b.ngroups == 0) return;
-  k_factor<TJ, TF><<<(b.ngroups + 3) / 4, 128, 0, s>>>(b, a);
+  k_factor<TJ, TF><<<(b.ngroups + 1) / 2, 128, 0, s>>>(b, a);
 }
 
 template void launch_face_jac<double>(const Batch&, const JacArgs&, cudaStream_t);

@@ -39,7 +39,7 @@ template <> struct SweepTypes<float> {
   using TF = __half;
   using TC = float;
   static constexpr int kStages = 4;   // bulk-copy ring stages per half
-  static constexpr int kAhead = 2;    // steps between loading a vector entry and its use
+  static constexpr int kAhead = 4;    // steps between loading a vector entry and its use
 };
 template <> struct SweepTypes<double> {
   using TF = double;

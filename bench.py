@@ -980,7 +980,7 @@ def main():
     ap.add_argument("--served-rate", type=float, default=50.0, help="request arrivals per second")
     ap.add_argument("--served-window", type=float, default=2.0, help="seconds of arrivals (0 skips)")
     ap.add_argument("--served-chains", type=int, default=3, help="continuation chains per alpha sweep")
-    ap.add_argument("--served-hbm-gb", type=float, default=4.0,
+    ap.add_argument("--served-hbm-gb", type=float, default=8.0,
                     help="workspace budget of the service (slots beyond those that saturate the GPU only "
                          "add latency)")
     ap.add_argument("--served-max-iter", type=int, default=100, help="Newton steps per point at most")
