@@ -57,6 +57,16 @@ __device__ __forceinline__ double gs_reduce_to_thread(double (&v)[NV], double* s
   return s;
 }
 
+// fixed-order sum of a per-chunk partial over a case's chunks (every lane gets it)
+__device__ __forceinline__ double warp_chunk_sum(const double* p, size_t stride, int nchunks) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int c = lane; c < nchunks; c += 32) s += p[(size_t)c * stride];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
 // s_q (h1_q [+ h2_q]) of the slice's vectors into shared memory
 template <typename TB>
 __device__ __forceinline__ void coef_to_smem(const GsArgs<TB>& a, int cs, int ncases, double* coef, bool both) {
@@ -65,6 +75,30 @@ __device__ __forceinline__ void coef_to_smem(const GsArgs<TB>& a, int cs, int nc
     double h = a.h1[(size_t)cs * kHStride + qq];
     if (both) h += a.h2[(size_t)cs * kHStride + qq];
     coef[q] = h * a.scale[(size_t)qq * ncases + cs];
+  }
+  __syncthreads();
+}
+
+// the same from the folded reduction: one warp per coefficient reduces the case's
+// chunk partials in k_gs_reduce's order; the case's first chunk stores the result
+template <typename TB>
+__device__ __forceinline__ void coef_folded(const GsArgs<TB>& a, const CaseDev& cs, int cs_id, int ncases,
+                                            bool first_chunk, double* coef, bool both) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nred = a.nq + (a.fold_wn0 != nullptr ? 1 : 0);
+  for (int q = warp; q < nred; q += blockDim.x >> 5) {
+    const double sum = warp_chunk_sum(a.fold_part + (size_t)cs.chunk0 * a.pstride + q, a.pstride, cs.nchunks);
+    if (lane == 0) {
+      if (q < a.nq) {
+        const double sc = a.scale[(size_t)q * ncases + cs_id];
+        const double h = sum * sc;
+        if (first_chunk) a.fold_h[(size_t)cs_id * kHStride + q] = h;
+        const double hh = both ? a.h1[(size_t)cs_id * kHStride + q] + h : h;
+        coef[q] = hh * sc;
+      } else if (first_chunk) {
+        a.fold_wn0[cs_id] = sqrt(sum);
+      }
+    }
   }
   __syncthreads();
 }
@@ -329,9 +363,10 @@ __global__ void __launch_bounds__(kGT) k_gs_project(Batch b, GsArgs<TB> a) {
   const Chunk ch = b.chunks[blockIdx.x];
   if (!case_live(b, ch.cs, a.need)) return;
   const CaseDev cs = b.cases[ch.cs];
-  coef_to_smem(a, ch.cs, b.ncases, coef, false);
   GsRing<TB> ring;
-  ring.init(smem, a, ch, 4 * cs.cell_off + ch.begin);
+  ring.init(smem, a, ch, 4 * cs.cell_off + ch.begin);   // the first bulk copies go out first
+  if (a.fold_part != nullptr) coef_folded(a, cs, ch.cs, b.ncases, ch.begin == 0, coef, false);
+  else coef_to_smem(a, ch.cs, b.ncases, coef, false);
   constexpr int EPT = GsRing<TB>::EPT;
   double acc[NQ];
 #pragma unroll
@@ -386,9 +421,10 @@ __global__ void __launch_bounds__(kGT) k_gs_sub(Batch b, GsArgs<TB> a) {
   if (!case_live(b, ch.cs, a.need)) return;
   const CaseDev cs = b.cases[ch.cs];
   const size_t base = 4 * cs.cell_off + ch.begin;
-  coef_to_smem(a, ch.cs, b.ncases, coef, a.both != 0);
   GsRing<TB> ring;
-  ring.init(smem, a, ch, base);
+  ring.init(smem, a, ch, base);   // the first bulk copies go out first
+  if (a.fold_part != nullptr) coef_folded(a, cs, ch.cs, b.ncases, ch.begin == 0, coef, a.both != 0);
+  else coef_to_smem(a, ch.cs, b.ncases, coef, a.both != 0);
   constexpr int EPT = GsRing<TB>::EPT;
   constexpr int E = GsRing<TB>::E;
   const int nq = a.nq;
@@ -459,15 +495,6 @@ __global__ void __launch_bounds__(kGB) k_gs_start(Batch b, GsArgs<TB> a) {
 
 // sum over a case's chunks of one partial, by one warp: lane c takes chunks
 // c, c+32, ... in order, then a fixed butterfly; every lane gets the total
-__device__ __forceinline__ double warp_chunk_sum(const double* p, size_t stride, int nchunks) {
-  const int lane = threadIdx.x & 31;
-  double s = 0.0;
-  for (int c = lane; c < nchunks; c += 32) s += p[(size_t)c * stride];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  return s;
-}
-
 // per-case reduction of the chunk partials: one block per case, one warp per coefficient
 __global__ void __launch_bounds__(256) k_gs_reduce(Batch b, GsReduceArgs a) {
   const int cs_id = blockIdx.x;
@@ -523,7 +550,7 @@ __global__ void __launch_bounds__(32) k_gs_close(Batch b, GsCloseArgs a) {
 // ---------------------------------------------------------------------------
 // host side: tier dispatch and the chained path for more than 32 vectors
 // ---------------------------------------------------------------------------
-constexpr int kSlice = 32;
+constexpr int kSlice = kGsSlice;
 
 #define A2D_GS_DISPATCH(KERNEL)                                                              \
   template <typename TB>                                                                     \

@@ -8,6 +8,7 @@
 namespace a2d {
 
 constexpr int kHStride = kMaxRestart + 2;   // per-case stride of coefficient arrays
+constexpr int kGsSlice = 32;                // basis vectors one pass handles (more: chained slices)
 
 template <typename TB>
 struct GsArgs {
@@ -30,6 +31,15 @@ struct GsArgs {
   double* part_norm = nullptr;    // per-chunk squared norm of the result
   uint32_t* err = nullptr;        // set to 1 when a bulk-copy wait runs out of time
   uint32_t need = 0;
+  // Folded per-case reduction (one slice, nq <= 32): when fold_part is set, every CTA
+  // reduces its case's chunk partials fold_part[chunk][q] itself (the order of
+  // k_gs_reduce) into this pass's coefficients, h_q = scale_q * sum, while its first
+  // bulk copies are in flight; the case's first chunk also stores h in fold_h (and, with
+  // fold_wn0, the norm of w from the partials' slot nq).  project: the coefficients are
+  // h1; sub (both): h1 from h1 plus the folded h2.
+  const double* fold_part = nullptr;
+  double* fold_h = nullptr;
+  double* fold_wn0 = nullptr;
 };
 
 struct GsReduceArgs {

@@ -91,7 +91,8 @@ struct a2d_plan {
   size_t o_vec[kNumVec] = {};
   size_t o_diag = 0, o_dt = 0, o_JIL = 0, o_JIR = 0, o_JJL = 0, o_JJR = 0, o_INV = 0, o_CF = 0, o_PQG = 0, o_V = 0;
   size_t o_H = 0, o_h1 = 0, o_h2 = 0, o_scale = 0, o_y = 0, o_wn0 = 0, o_circ = 0, o_circ_rk = 0;
-  size_t o_tpart = 0, o_cpart = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0, o_cnt = 0, o_idx = 0;
+  size_t o_tpart = 0, o_cpart = 0, o_cpart2 = 0, o_cpartn = 0, o_coef = 0, o_cp = 0, o_hrn = 0, o_hcl = 0,
+         o_cnt = 0, o_idx = 0;
   size_t o_sat = 0;        // saturated FP16 factor entries since bind (a2d_factor_saturations)
   size_t o_jtiles = 0;
   Batch jbatch{};          // the batch with the JVP's tile list
@@ -206,6 +207,7 @@ static void layout(a2d_plan* P) {
   P->o_tpart = cv.take(8 * kTilePartStride * P->tiles.size());
   P->pstride = P->m + 2;
   P->o_cpart = cv.take(8 * (size_t)P->pstride * P->chunks.size());
+  P->o_cpart2 = cv.take(8 * (size_t)P->pstride * P->chunks.size());   // pass-2 partials of the folded path
   P->o_cpartn = cv.take(8 * P->chunks.size());
   P->o_coef = cv.take(8 * 3 * (size_t)B);
   P->o_cp = cv.take(8 * (size_t)P->total_ni);
@@ -547,20 +549,35 @@ static void newton_step_launches(a2d_plan* P, cudaStream_t s) {
     g.need = KR;
     g.with_norm = 1;
     launch_gs_dots<TB>(B, g, s);
-    GsReduceArgs rd;
-    rd.part = cpart;
-    rd.pstride = P->pstride;
-    rd.nq = k + 1;
-    rd.scale = scale;
-    rd.h = h1;
-    rd.wn0 = wn0;
-    rd.need = KR;
-    launch_gs_reduce(B, rd, s);
-    launch_gs_project<TB>(B, g, s);
-    rd.h = h2;
-    rd.wn0 = nullptr;
-    launch_gs_reduce(B, rd, s);
-    launch_gs_finish<TB>(B, g, s);
+    if (k + 1 <= kGsSlice) {
+      // one slice: the per-case reductions run inside the next pass (no reduce launches);
+      // pass 2 writes its partials to a second buffer while it reads pass 1's
+      GsArgs<TB> gp = g;
+      gp.fold_part = cpart;
+      gp.fold_h = h1;
+      gp.fold_wn0 = wn0;
+      gp.part = P->at<double>(P->o_cpart2);
+      launch_gs_project<TB>(B, gp, s);
+      GsArgs<TB> gf = g;
+      gf.fold_part = P->at<double>(P->o_cpart2);
+      gf.fold_h = h2;
+      launch_gs_finish<TB>(B, gf, s);
+    } else {
+      GsReduceArgs rd;
+      rd.part = cpart;
+      rd.pstride = P->pstride;
+      rd.nq = k + 1;
+      rd.scale = scale;
+      rd.h = h1;
+      rd.wn0 = wn0;
+      rd.need = KR;
+      launch_gs_reduce(B, rd, s);
+      launch_gs_project<TB>(B, g, s);
+      rd.h = h2;
+      rd.wn0 = nullptr;
+      launch_gs_reduce(B, rd, s);
+      launch_gs_finish<TB>(B, g, s);
+    }
     GsCloseArgs ck;
     ck.part_norm = cpartn;
     ck.wn0 = wn0;
