@@ -191,50 +191,4 @@ __device__ __forceinline__ Dual<T, N> vmax(const Dual<T, N>& a, T b) {
 template <typename S>
 __device__ __forceinline__ S sel(bool c, const S& a, const S& b) { return c ? a : b; }
 
-#ifdef A2D_PACKED_DUAL
-// One-tangent FP32 dual numbers on the packed FP32 pipe of sm_100a (f32x2: two
-// lanes per instruction): the value and the tangent of a sum, a difference or a
-// scaling by a real are one instruction, a product two.  Flush-to-zero rounding,
-// as the translation unit that defines this compiles its FP32 arithmetic.
-__device__ __forceinline__ unsigned long long dpack(const Dual<float, 1>& a) {
-  unsigned long long r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.v), "f"(a.d[0]));
-  return r;
-}
-__device__ __forceinline__ Dual<float, 1> dunpack(unsigned long long r) {
-  Dual<float, 1> a;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.v), "=f"(a.d[0]) : "l"(r));
-  return a;
-}
-__device__ __forceinline__ unsigned long long dsplat(float c) {
-  unsigned long long r;
-  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(c));
-  return r;
-}
-__device__ __forceinline__ Dual<float, 1> operator+(const Dual<float, 1>& a, const Dual<float, 1>& b) {
-  unsigned long long r;
-  asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(dpack(a)), "l"(dpack(b)));
-  return dunpack(r);
-}
-__device__ __forceinline__ Dual<float, 1> operator-(const Dual<float, 1>& a, const Dual<float, 1>& b) {
-  unsigned long long r;
-  asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(dpack(a)), "l"(dpack(b)));
-  return dunpack(r);
-}
-// (a.v b.v, a.d b.v) in one instruction, then a.d b.v + a.v b.d
-__device__ __forceinline__ Dual<float, 1> operator*(const Dual<float, 1>& a, const Dual<float, 1>& b) {
-  unsigned long long r;
-  asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(dpack(a)), "l"(dsplat(b.v)));
-  Dual<float, 1> p = dunpack(r);
-  p.d[0] = fmaf(a.v, b.d[0], p.d[0]);
-  return p;
-}
-__device__ __forceinline__ Dual<float, 1> operator*(const Dual<float, 1>& a, float c) {
-  unsigned long long r;
-  asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(dpack(a)), "l"(dsplat(c)));
-  return dunpack(r);
-}
-__device__ __forceinline__ Dual<float, 1> operator*(float c, const Dual<float, 1>& a) { return a * c; }
-#endif
-
 }  // namespace a2d

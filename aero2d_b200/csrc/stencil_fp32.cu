@@ -7,7 +7,6 @@
 // ulp off round-to-nearest are immaterial to the result.
 #include <cuda_bf16.h>
 
-#define A2D_PACKED_DUAL 1   // one-tangent duals on the packed FP32 pipe (dual.cuh)
 #include "stencil_impl.cuh"
 
 namespace a2d {
