@@ -126,6 +126,10 @@ SIGNATURES = {
     "a2d_service_destroy": (_I, [_P]),
     "a2d_service_stats": (_I, [_P, C.POINTER(_I), C.POINTER(C.c_longlong)]),
     "a2d_service_plan": (_I, [_P, C.POINTER(_P)]),
+    "a2d_service_lanes": (_I, [_P, C.POINTER(_I)]),
+    "a2d_service_lane": (_I, [_P, _I, C.POINTER(_P), C.POINTER(_I), C.POINTER(_I)]),
+    "a2d_service_create_lanes": (_I, [_I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_P), C.POINTER(_I), _I,
+                                      C.POINTER(Params), C.POINTER(_P)]),
     "a2d_plan_set_coarse": (_I, [_P, _P]),
     "a2d_case_set_grid": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_P), _P]),
     "a2d_service_create_ragged": (_I, [_I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_P), C.POINTER(_I),

@@ -75,11 +75,14 @@ class EulerService:
     def __init__(self, grid: OGrid | DeviceGrid | None = None, slots: int = 64, dtype=np.float32, device=None,
                  tol: float = 1e-8, max_iter: int = 200, gmres_restart: int = 30, cfl0: float = 10.0,
                  cfl_max: float = 300.0, gmres_tol: float = 0.01, jacobi_sweeps: int = 4,
-                 max_update: float = 0.2, classes: Optional[Sequence[tuple]] = None, tuning="cached"):
+                 max_update: float = 0.2, classes: Optional[Sequence[tuple]] = None, tuning="cached",
+                 lanes: Optional[int] = None):
         """`grid` + `slots` for one grid size, or `classes` = [(grid, slots), ...]
         with one grid per size (the class's default grid).  `tuning` as for
         plan.Plan: "cached", "auto" (measured on the idle slots at creation on a
-        cache miss), None, or a (jvp_tile, sweep) pair."""
+        cache miss), None, or a (jvp_tile, sweep) pair.  `lanes`: plans the slots
+        are dealt to, stepped concurrently on their own streams (default: one per
+        16 slots of the largest class, at most 4)."""
         if classes is None:
             if grid is None:
                 raise ValueError("give a grid (and slots) or classes")
@@ -101,12 +104,17 @@ class EulerService:
             setattr(p, k, v)
         self.lib = _lib.load()
         m = len(self.classes)
+        if lanes is None:
+            lanes = default_lanes([n for _, n in self.classes])
         h = C.c_void_p()
-        _lib.check(self.lib.a2d_service_create_ragged(
+        _lib.check(self.lib.a2d_service_create_lanes(
             m, (C.c_int * m)(*[s[0] for s in shapes]), (C.c_int * m)(*[s[1] for s in shapes]),
             (C.c_void_p * m)(*[dg.ptr for dg, _ in self.classes]), (C.c_int * m)(*[n for _, n in self.classes]),
-            C.byref(p), C.byref(h)))
+            int(lanes), C.byref(p), C.byref(h)))
         self.handle = h
+        nl = C.c_int()
+        _lib.check(self.lib.a2d_service_lanes(h, C.byref(nl)))
+        self.lanes = nl.value
         n = C.c_size_t()
         _lib.check(self.lib.a2d_service_workspace_bytes(h, C.byref(n)))
         self.workspace_bytes = n.value
@@ -119,9 +127,9 @@ class EulerService:
             self._tune(tuning)
 
     def _tune(self, tuning) -> None:
-        """Applies (or, with "auto" on a cache miss, measures) the launch
-        configuration on the service's own plan while every slot is idle, then
-        retires every slot again."""
+        """Applies (or, with "auto" on a cache miss, measures on the first lane's
+        plan) the launch configuration of every lane while every slot is idle,
+        then retires every slot again."""
         from . import autotune
         view = _PlanView(self)
         if isinstance(tuning, str):
@@ -230,21 +238,39 @@ class EulerService:
         return done
 
 
+def default_lanes(class_slots: Sequence[int]) -> int:
+    """Lanes of a service: one per 16 slots of its largest class, 1 to 4 (four
+    16-case plans of the 256 x 64 benchmark step 6 % faster than one 64-case plan)."""
+    return max(1, min(4, max(class_slots) // 16))
+
+
 class _PlanView:
-    """The service's own plan, seen as a plan.Plan by the autotuner."""
+    """The service's first lane's plan, seen as a plan.Plan by the autotuner;
+    a launch configuration set through it is set on every lane."""
 
     def __init__(self, svc: "EulerService"):
-        h = C.c_void_p()
-        _lib.check(svc.lib.a2d_service_plan(svc.handle, C.byref(h)))
-        self.handle, self.lib, self.device, self.params = h, svc.lib, svc.device, svc._params
-        self.shapes = [(dg.ni, dg.nc) for dg, n in svc.classes for _ in range(n)]
+        self.lib, self.device, self.params = svc.lib, svc.device, svc._params
+        slot_shape = [(dg.ni, dg.nc) for dg, n in svc.classes for _ in range(n)]
+        self.handles = []
+        for lane in range(svc.lanes):
+            h, n = C.c_void_p(), C.c_int()
+            _lib.check(svc.lib.a2d_service_lane(svc.handle, lane, C.byref(h), C.byref(n), None))
+            if lane == 0:
+                ids = (C.c_int * n.value)()
+                _lib.check(svc.lib.a2d_service_lane(svc.handle, 0, None, None, ids))
+                self.shapes = [slot_shape[k] for k in ids]
+            self.handles.append(h)
+        self.handle = self.handles[0]
 
     def _call(self, name, *args):
         with torch.cuda.device(self.device):
             _lib.check(getattr(self.lib, name)(self.handle, *args, stream_handle(self.device)))
 
     def set_tuning(self, jvp_tile: str = "32x8", sweep: str = "lanes") -> None:
-        self._call("a2d_plan_set_tuning", _lib.JVP_TILES[jvp_tile], _lib.SWEEP_VARIANTS[sweep])
+        with torch.cuda.device(self.device):
+            for h in self.handles:
+                _lib.check(self.lib.a2d_plan_set_tuning(h, _lib.JVP_TILES[jvp_tile], _lib.SWEEP_VARIANTS[sweep],
+                                                        stream_handle(self.device)))
 
     def tuning(self) -> tuple[str, str]:
         t, v = C.c_int(), C.c_int()
@@ -260,4 +286,4 @@ class _PlanView:
 
     def retire_all(self) -> None:
         n = len(self.shapes)
-        self._call("a2d_case_retire", n, (C.c_int * n)(*range(n)))
+        self._call("a2d_case_retire", n, (C.c_int * n)(*range(n)))   # the first lane's cases

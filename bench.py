@@ -411,7 +411,7 @@ def gpu_arm(args, rank: int, world: int, dist):
 
     def make_service(g, dtype=np.float32):
         return EulerService(g, slots=B, dtype=dtype, device=dev, tol=args.tol, max_iter=args.max_iter,
-                            gmres_restart=args.restart, tuning="auto")
+                            gmres_restart=args.restart, tuning="auto", lanes=args.lanes)
 
     def barrier():
         if dist is not None:
@@ -435,7 +435,7 @@ def gpu_arm(args, rank: int, world: int, dist):
     converged = int(reached.sum())
     kps, steps_after = svc.stats()
     # per Newton step: the graph's kernels and the service's status/forces/restart kernels
-    launches = (steps_after - steps_before) * (kps + 3)
+    launches = (steps_after - steps_before) * (kps + 3 * svc.lanes)
     elapsed_ms, converged_all = replicas.job_time_and_count(elapsed_ms, converged, dist, dev)
     converged_all = int(converged_all)
     value = converged_all / (elapsed_ms / 1e3)
@@ -451,8 +451,9 @@ def gpu_arm(args, rank: int, world: int, dist):
                      "arithmetic; FP16 sweep factors; BF16 Krylov basis",
         "parallelism": f"replicas x{world}, case sharding",
         "mode": f"served stream: the {args.steps} steps' {args.steps * B} cases queued at once into a {B}-slot "
-                "continuous-batching service (a case is admitted as soon as a slot retires; the batch drains once, "
-                "at the end of the stream)",
+                f"continuous-batching service ({svc.lanes} lanes of {B // svc.lanes} slots, each lane's plan stepped "
+                "on its own stream, concurrently; a case is admitted as soon as a slot retires; the batch drains "
+                "once, at the end of the stream)",
         "tuning": {"jvp_tile": tuning[0], "sweep": tuning[1],
                    "note": "chosen by aero2d_b200.autotune on this GPU (timed Newton steps of every configuration)"},
         "converged_cases": converged_all,
@@ -545,7 +546,7 @@ def gpu_arm(args, rank: int, world: int, dist):
     torch.cuda.synchronize()
     t = time.perf_counter()
     svc_e = EulerService(grid, slots=B, dtype=np.float32, device=dev, tol=args.tol, max_iter=args.max_iter,
-                         gmres_restart=args.restart)
+                         gmres_restart=args.restart, lanes=args.lanes)
     ids = [svc_e.submit(float(m), [float(a)], continuation=False) for m, a in zip(sm, sa)]
     svc_e.run()
     res_e = [svc_e.result(rid) for rid in ids]
@@ -965,6 +966,8 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--cases", type=int, default=CASES)
     ap.add_argument("--restart", type=int, default=RESTART)
+    ap.add_argument("--lanes", type=int, default=None,
+                    help="service lanes (plans stepped concurrently; default: the service's, 4 for 64 slots)")
     ap.add_argument("--tol", type=float, default=TOL)
     ap.add_argument("--max-iter", type=int, default=MAX_ITER)
     ap.add_argument("--single-sample", type=int, default=4)

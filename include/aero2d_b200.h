@@ -193,6 +193,13 @@ int a2d_service_create(int ni, int nc, const void* metrics, int slots, const a2d
  * the class's default grid (used by a2d_service_submit and by requests without a grid) */
 int a2d_service_create_ragged(int nclasses, const int* ni, const int* nc, const void* const* metrics,
                               const int* slots, const a2d_params* params, a2d_service** service);
+/* the same with the slots split into `lanes` plans (at most the largest class's slot count):
+ * slot q of each class goes to lane q mod lanes; a Newton step of every busy lane runs on the
+ * lane's own stream, forked from and joined back into the caller's, so that the lanes'
+ * kernels overlap on the GPU.  Results do not depend on the lane count (lanes = 1: one plan
+ * stepped on the caller's stream, as a2d_service_create_ragged) */
+int a2d_service_create_lanes(int nclasses, const int* ni, const int* nc, const void* const* metrics,
+                             const int* slots, int lanes, const a2d_params* params, a2d_service** service);
 int a2d_service_workspace_bytes(const a2d_service* service, size_t* bytes);
 int a2d_service_bind(a2d_service* service, void* workspace, size_t bytes, void* stream);
 /* a request on the first class's default grid; winf: host [npoints][4]; *id receives the
@@ -216,11 +223,16 @@ int a2d_service_result(a2d_service* service, long long id, double* coef, double*
  * a2d_service_result, which releases the request */
 int a2d_service_result_drop(a2d_service* service, long long id, double* drop);
 int a2d_service_pending(a2d_service* service, int* queued, int* running);
-/* the service's own plan (borrowed; it lives as long as the service): its slots in class
- * order, for a2d_plan_set_tuning and the measurement calls.  Stepping it directly, outside
- * a2d_service_step, is only safe while no request is queued or running */
+/* the service's first lane's plan (borrowed; it lives as long as the service; with one lane
+ * its slots are the service's in class order), for a2d_plan_set_tuning and the measurement
+ * calls.  Stepping a lane's plan directly, outside a2d_service_step, is only safe while no
+ * request is queued or running */
 int a2d_service_plan(a2d_service* service, a2d_plan** plan);
-/* kernel launches of one Newton step of the service's plan (counted in its captured graph; 0
+/* the number of lanes, and one lane's plan (borrowed), case count and the service slot of
+ * each of its cases (slots: an array of nslots, or NULL) */
+int a2d_service_lanes(const a2d_service* service, int* lanes);
+int a2d_service_lane(a2d_service* service, int lane, a2d_plan** plan, int* nslots, int* slots);
+/* kernel launches of one Newton step of all lanes' plans (counted in their captured graphs; 0
  * before the first step) and the Newton steps the service has taken since bind */
 int a2d_service_stats(a2d_service* service, int* kernels_per_step, long long* newton_steps);
 int a2d_service_destroy(a2d_service* service);

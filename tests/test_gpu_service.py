@@ -135,3 +135,32 @@ def test_ragged_service_alone_and_in_the_mix(cuda, dtype):
         for key in ("cl", "cd", "cm", "cp", "converged", "nsteps"):
             assert np.array_equal(ra[key], rm[key]), key
     mix.close()
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_service_lanes_same_results(cuda, dtype):
+    """The slots dealt to three lanes (three plans stepped concurrently on their
+    own streams, forked from and joined into the caller's): every request's
+    points are bitwise the same as with one lane, and the ragged classes are
+    dealt to every lane."""
+    from aero2d_b200.geometry import naca4
+    from aero2d_b200.gridgen import ogrid_batch
+    small = ogrid_batch([naca4(c, 33) for c in ("0012", "2412", "4415")], nj=25, ds0=2e-3, radius=20.0, device=cuda)
+    large = ogrid_batch([naca4(c, 49) for c in ("0012", "2412")], nj=33, ds0=2e-3, radius=20.0, device=cuda)
+    reqs = [(small[0], 0.5, [0.0, 2.0], True), (large[0], 0.6, [1.0, 3.0], True), (small[1], 0.4, [4.0], False),
+            (small[2], 0.55, [-2.0, 0.0, 2.0], True), (large[1], 0.3, [2.0], True), (small[0], 0.45, [1.0], True),
+            (large[0], 0.5, [0.0, -1.0], True)]
+    kw = dict(dtype=dtype, device=cuda, tol=1e-8, max_iter=120)
+    out = {}
+    for lanes in (1, 3):
+        svc = EulerService(classes=[(small[0], 4), (large[0], 3)], lanes=lanes, **kw)
+        assert svc.lanes == lanes
+        ids = [svc.submit(m, a, continuation=c, grid=g) for g, m, a, c in reqs]
+        done = svc.run()
+        assert sorted(done) == sorted(ids)
+        assert svc.pending() == (0, 0)
+        out[lanes] = [svc.result(rid) for rid in ids]
+        svc.close()
+    for r1, r3 in zip(out[1], out[3]):
+        for key in ("cl", "cd", "cm", "cp", "converged", "nsteps", "drop"):
+            assert np.array_equal(r1[key], r3[key], equal_nan=True), key
