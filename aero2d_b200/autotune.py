@@ -127,7 +127,11 @@ def device_key(device) -> str:
 
 
 def plan_key(plan) -> str:
-    return device_key(plan.device) + "|" + signature(plan.shapes, plan.params.precision)
+    """The cache key of a plan (a service's lanes: the first lane's cases and the
+    lane count, since the lanes are timed stepping together)."""
+    lanes = int(getattr(plan, "lanes", 1))
+    return (device_key(plan.device) + "|" + signature(plan.shapes, plan.params.precision) +
+            (f"|lanes{lanes}" if lanes > 1 else ""))
 
 
 def time_newton_steps(plan, steps: int = 2) -> float:

@@ -245,13 +245,16 @@ def default_lanes(class_slots: Sequence[int]) -> int:
 
 
 class _PlanView:
-    """The service's first lane's plan, seen as a plan.Plan by the autotuner;
-    a launch configuration set through it is set on every lane."""
+    """The service's lanes seen as one plan.Plan by the autotuner: a launch
+    configuration is set on every lane, and a Newton step steps every lane
+    concurrently on its own stream (as a2d_service_step does), so that the
+    configuration is timed under the load it will serve.  `shapes` are the first
+    lane's cases and `lanes` the lane count (both part of the tuning key)."""
 
     def __init__(self, svc: "EulerService"):
         self.lib, self.device, self.params = svc.lib, svc.device, svc._params
         slot_shape = [(dg.ni, dg.nc) for dg, n in svc.classes for _ in range(n)]
-        self.handles = []
+        self.handles, self.counts = [], []
         for lane in range(svc.lanes):
             h, n = C.c_void_p(), C.c_int()
             _lib.check(svc.lib.a2d_service_lane(svc.handle, lane, C.byref(h), C.byref(n), None))
@@ -260,17 +263,18 @@ class _PlanView:
                 _lib.check(svc.lib.a2d_service_lane(svc.handle, 0, None, None, ids))
                 self.shapes = [slot_shape[k] for k in ids]
             self.handles.append(h)
+            self.counts.append(n.value)
         self.handle = self.handles[0]
+        self.lanes = len(self.handles)
+        self._streams = None
 
-    def _call(self, name, *args):
-        with torch.cuda.device(self.device):
-            _lib.check(getattr(self.lib, name)(self.handle, *args, stream_handle(self.device)))
-
-    def set_tuning(self, jvp_tile: str = "32x8", sweep: str = "lanes") -> None:
+    def _each(self, name, *args):
         with torch.cuda.device(self.device):
             for h in self.handles:
-                _lib.check(self.lib.a2d_plan_set_tuning(h, _lib.JVP_TILES[jvp_tile], _lib.SWEEP_VARIANTS[sweep],
-                                                        stream_handle(self.device)))
+                _lib.check(getattr(self.lib, name)(h, *args, stream_handle(self.device)))
+
+    def set_tuning(self, jvp_tile: str = "32x8", sweep: str = "lanes") -> None:
+        self._each("a2d_plan_set_tuning", _lib.JVP_TILES[jvp_tile], _lib.SWEEP_VARIANTS[sweep])
 
     def tuning(self) -> tuple[str, str]:
         t, v = C.c_int(), C.c_int()
@@ -279,11 +283,24 @@ class _PlanView:
                 {b: a for a, b in _lib.SWEEP_VARIANTS.items()}[v.value])
 
     def init_freestream(self) -> None:
-        self._call("a2d_init_freestream")
+        self._each("a2d_init_freestream")
 
     def newton_step(self) -> None:
-        self._call("a2d_newton_step")
+        with torch.cuda.device(self.device):
+            if self.lanes == 1:
+                _lib.check(self.lib.a2d_newton_step(self.handle, stream_handle(self.device)))
+                return
+            if self._streams is None:
+                self._streams = [torch.cuda.Stream(self.device) for _ in self.handles]
+            cur = torch.cuda.current_stream(self.device)
+            fork = torch.cuda.Event()
+            fork.record(cur)
+            for h, st in zip(self.handles, self._streams):
+                st.wait_event(fork)
+                _lib.check(self.lib.a2d_newton_step(h, st.cuda_stream))
+                cur.wait_stream(st)
 
     def retire_all(self) -> None:
-        n = len(self.shapes)
-        self._call("a2d_case_retire", n, (C.c_int * n)(*range(n)))   # the first lane's cases
+        with torch.cuda.device(self.device):
+            for h, n in zip(self.handles, self.counts):
+                _lib.check(self.lib.a2d_case_retire(h, n, (C.c_int * n)(*range(n)), stream_handle(self.device)))

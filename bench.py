@@ -811,7 +811,7 @@ def served_arm(args, dev):
     defaults = [ogrid_batch([naca4("0012", ns)], nj=nj, ds0=ds0, radius=20.0, device=dev)[0]
                 for ns, nj, ds0 in SERVED_SIZES]
     svc = EulerService(classes=list(zip(defaults, slots)), dtype=np.float32, device=dev, tol=1e-8,
-                       max_iter=args.served_max_iter, gmres_restart=RESTART, tuning="auto")
+                       max_iter=args.served_max_iter, gmres_restart=RESTART, tuning="auto", lanes=args.lanes)
     w = svc.submit(0.5, [2.0], grid=defaults[0])
     svc.run()
     svc.result(w)
@@ -892,7 +892,8 @@ def served_arm(args, dev):
                     "(128x32, 192x48, 256x64, 384x96), M~U[0.2,0.75], mixed precision, drop 1e-8, at most "
                     f"{args.served_max_iter} Newton steps per point, the sweep as {len(chains)} continuation chains "
                     "in parallel slots, grids generated on the device on arrival",
-        "slots": dict(zip([f"{a}x{b}" for a, b in shapes], slots)), "hbm_budget_gb": args.served_hbm_gb,
+        "slots": dict(zip([f"{a}x{b}" for a, b in shapes], slots)), "lanes": svc.lanes,
+        "hbm_budget_gb": args.served_hbm_gb,
         "requests_done": len(done_at), "requests_offered": n, "grid_rejections": rejected,
         "latency_s": pct(lat), "points": pts, "points_reached_1e-8": reach, "converged_points": conv,
         "converged_points_per_s": round(conv / span, 3) if done_at else None,

@@ -84,3 +84,16 @@ def test_tune_and_apply_with_a_fake_timer(tmp_path, monkeypatch):
     assert autotune.apply(fresh, measure=True, cache=cache, measure_fn=measure) == ("16x16", "rows")
     again = FakePlan()
     assert autotune.apply(again, measure=False, cache=cache) == ("16x16", "rows") and again.inits == 0
+
+
+def test_plan_key_counts_lanes(monkeypatch):
+    """A service's lanes are tuned stepping together: the lane count is part of
+    the key, so a 4 x 16-case service and a lone 16-case plan keep separate
+    configurations."""
+    from types import SimpleNamespace
+    monkeypatch.setattr(autotune, "device_key", lambda device: "gpu|lib")
+    plan = SimpleNamespace(device=None, shapes=[(256, 64)] * 16, params=SimpleNamespace(precision=1))
+    lone = autotune.plan_key(plan)
+    plan.lanes = 4
+    assert lone == "gpu|lib|mixed|256x64:16"
+    assert autotune.plan_key(plan) == lone + "|lanes4"
