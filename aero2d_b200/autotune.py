@@ -36,7 +36,7 @@ from typing import Callable, Iterable, Optional
 
 JVP_TILES = ("32x8", "32x16", "64x4", "16x16")
 SWEEPS = ("lanes", "rows", "pairs")
-DEFAULT = ("32x8", "lanes")
+DEFAULT = ("32x16", "rows")   # a new plan's configuration (the library's defaults)
 
 
 def default_path() -> Path:

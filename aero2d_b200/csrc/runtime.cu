@@ -77,8 +77,10 @@ struct a2d_plan {
   std::vector<CaseDev> cases;
   std::vector<Tile> tiles;
   std::vector<Tile> jtiles;    // tiles of the FP32 linearised stencil, in the shape jvp_tile
-  int jvp_tile = kTile32x8;    // tuning knobs (a2d_plan_set_tuning)
-  int sweep_variant = kSweepLanes;
+  // tuning knobs (a2d_plan_set_tuning); the defaults are the autotuner's choice on every
+  // batch shape measured on a B200 (64 and 4 x 16 cases of 256 x 64, the ragged sets)
+  int jvp_tile = kTile32x16;
+  int sweep_variant = kSweepRows;
   int max_jtiles = 0;          // the most tiles any JVP tile shape needs (workspace room)
   std::vector<Chunk> chunks;
   std::vector<Group> groups;

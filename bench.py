@@ -407,7 +407,7 @@ def gpu_arm(args, rank: int, world: int, dist):
         base = EulerSolver(grid, dtype=dtype, device=dev)
         s = ImplicitEuler(base, gmres_restart=args.restart)
         winf = base.freestream(cases_m, cases_a)
-        return Plan([base.dgrid] * len(cases_m), winf, s.params(args.tol, args.max_iter), dev), base
+        return Plan([base.dgrid] * len(cases_m), winf, s.params(args.tol, args.max_iter), dev, tuning="auto"), base
 
     def make_service(g, dtype=np.float32):
         return EulerService(g, slots=B, dtype=dtype, device=dev, tol=args.tol, max_iter=args.max_iter,
@@ -459,6 +459,8 @@ def gpu_arm(args, rank: int, world: int, dist):
         "converged_cases": converged_all,
         "cases_total": B * args.steps * world,
         "newton_steps_mean": round(float(np.mean([r["nsteps"][0] for r in res])), 2),
+        "service_steps": int(nsteps_run),
+        "ms_per_service_step": round(elapsed_ms / max(1, nsteps_run), 3),
         "latency_ms": dict(pct(svc_ms[reached], nd=2) or {},
                            note="per converged case, from its admission into a slot to its retirement"),
     }

@@ -19,7 +19,7 @@ def test_candidates_by_precision():
     mixed = autotune.candidates(1)
     assert len(mixed) == len(autotune.JVP_TILES) * len(autotune.SWEEPS)
     assert set(t for t, _ in autotune.candidates(0)) == {"32x8"}
-    assert mixed[0] == autotune.DEFAULT
+    assert autotune.DEFAULT in mixed
 
 
 def test_cache_roundtrip_and_bad_files(tmp_path):
