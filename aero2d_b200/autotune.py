@@ -63,9 +63,11 @@ def signature(shapes: Iterable[tuple[int, int]], precision: int) -> str:
 
 def candidates(precision: int) -> list[tuple[str, str]]:
     """Every configuration worth timing: the JVP tile shapes matter only in
-    the mixed precision (the FP64 JVP always runs 32 x 8 tiles)."""
-    tiles = JVP_TILES if precision else JVP_TILES[:1]
-    return [(t, v) for t in tiles for v in SWEEPS]
+    the mixed precision (the FP64 JVP always runs 32 x 8 tiles), and the rows
+    sweep runs mixed-precision plans only."""
+    if precision:
+        return [(t, v) for t in JVP_TILES for v in SWEEPS]
+    return [(JVP_TILES[0], v) for v in SWEEPS if v != "rows"]
 
 
 class TuningCache:

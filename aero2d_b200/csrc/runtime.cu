@@ -78,7 +78,8 @@ struct a2d_plan {
   std::vector<Tile> tiles;
   std::vector<Tile> jtiles;    // tiles of the FP32 linearised stencil, in the shape jvp_tile
   // tuning knobs (a2d_plan_set_tuning); the defaults are the autotuner's choice on every
-  // batch shape measured on a B200 (64 and 4 x 16 cases of 256 x 64, the ragged sets)
+  // batch shape measured on a B200 (64 and 4 x 16 cases of 256 x 64, the ragged sets); FP64
+  // plans start with the lanes sweep
   int jvp_tile = kTile32x16;
   int sweep_variant = kSweepRows;
   int max_jtiles = 0;          // the most tiles any JVP tile shape needs (workspace room)
@@ -734,6 +735,7 @@ int a2d_plan_create(int ncases, const int* ni, const int* nc, const void* const*
   }
   a2d_plan* P = new a2d_plan();
   P->p = p;
+  if (p.precision != A2D_MIXED) P->sweep_variant = kSweepLanes;   // rows runs mixed plans only
   P->ncases = ncases;
   P->m = p.gmres_restart;
   P->tj = p.precision == A2D_MIXED ? 4 : 8;
@@ -758,6 +760,8 @@ int a2d_plan_set_tuning(a2d_plan* P, int jvp_tile, int sweep_variant, void* stre
   if (jvp_tile < 0 || jvp_tile >= kNumTileShapes) return fail(A2D_ERR_ARG, "set_tuning: unknown JVP tile shape");
   if (sweep_variant < 0 || sweep_variant >= kNumSweepVariants)
     return fail(A2D_ERR_ARG, "set_tuning: unknown sweep variant");
+  if (sweep_variant == kSweepRows && P->p.precision != A2D_MIXED)
+    return fail(A2D_ERR_ARG, "set_tuning: the rows sweep runs mixed-precision plans only");
   if (jvp_tile != P->jvp_tile) {
     P->jvp_tile = jvp_tile;
     P->jtiles = tile_list(P, jvp_tile);

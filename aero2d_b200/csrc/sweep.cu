@@ -452,9 +452,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
 template <typename TI, bool FIRST>
 void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s, int variant) {
   if (b.ngroups == 0) return;
-  if (variant == kSweepRows) {
-    launch_sweep_rows<TI, FIRST>(b, a, last, s);
-    return;
+  if constexpr (sizeof(TI) == 4) {   // the rows variant runs mixed-precision plans only
+    if (variant == kSweepRows) {
+      launch_sweep_rows<TI, FIRST>(b, a, last, s);
+      return;
+    }
   }
   if (variant == kSweepPairs) {
     launch_sweep_pairs<TI, FIRST>(b, a, last, s);

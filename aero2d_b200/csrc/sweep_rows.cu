@@ -13,7 +13,10 @@
 // they are used; the halves meet twice around the twist row.  Four warps per
 // line half spread a step's arithmetic over more threads than the lane variant
 // (a plan's tuning knob picks one, aero2d_b200.autotune).  The row arithmetic is
-// the same as the lane variant's, in the same order.  Every wait is bounded; a
+// the same as the lane variant's, in the same order.  Mixed-precision plans only:
+// an FP64 form gave results that depended on which other cases shared the batch
+// (deterministic for a given batch; the cause was not found), so FP64 plans run
+// the lane or pair variants, whose results are independent of the batch.  Every wait is bounded; a
 // wait that runs out records an error and the CTA drains its copies in flight
 // (bounded again) before exit.
 #include <type_traits>
@@ -40,12 +43,6 @@ template <> struct SweepTypes<float> {
   using TC = float;
   static constexpr int kStages = 4;   // bulk-copy ring stages per half
   static constexpr int kAhead = 4;    // steps between loading a vector entry and its use
-};
-template <> struct SweepTypes<double> {
-  using TF = double;
-  using TC = double;
-  static constexpr int kStages = 2;
-  static constexpr int kAhead = 2;
 };
 
 template <typename TI>
@@ -85,11 +82,6 @@ __device__ __forceinline__ void load4(const double* p, float (&v)[4]) {
   const double2 t0 = *reinterpret_cast<const double2*>(p);
   const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
   v[0] = (float)t0.x; v[1] = (float)t0.y; v[2] = (float)t1.x; v[3] = (float)t1.y;
-}
-__device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
-  const double2 t0 = *reinterpret_cast<const double2*>(p);
-  const double2 t1 = *reinterpret_cast<const double2*>(p + 2);
-  v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
 }
 
 // barrier of the 128 consumer threads of one half (ids 1, 2) and of all 256
@@ -466,15 +458,11 @@ cudaError_t sweep_rows_init() {
 #define A2D_SWEEP_ATTR(TI, F, L) set(reinterpret_cast<const void*>(&k_sweep<TI, F, L>), sizeof(SweepSmem<TI>));
   A2D_SWEEP_ATTR(float, true, true) A2D_SWEEP_ATTR(float, true, false)
   A2D_SWEEP_ATTR(float, false, true) A2D_SWEEP_ATTR(float, false, false)
-  A2D_SWEEP_ATTR(double, true, true) A2D_SWEEP_ATTR(double, true, false)
-  A2D_SWEEP_ATTR(double, false, true) A2D_SWEEP_ATTR(double, false, false)
 #undef A2D_SWEEP_ATTR
   return e;
 }
 
 template void launch_sweep_rows<float, true>(const Batch&, const SweepArgs&, bool, cudaStream_t);
 template void launch_sweep_rows<float, false>(const Batch&, const SweepArgs&, bool, cudaStream_t);
-template void launch_sweep_rows<double, true>(const Batch&, const SweepArgs&, bool, cudaStream_t);
-template void launch_sweep_rows<double, false>(const Batch&, const SweepArgs&, bool, cudaStream_t);
 
 }  // namespace a2d

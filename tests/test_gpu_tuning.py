@@ -53,3 +53,13 @@ def test_autotuner_measures_stores_and_reapplies(cuda, tmp_path, monkeypatch):
     assert len(cache.load()[key]["ms"]) == len(autotune.candidates(_lib.A2D_MIXED))
     pl2 = ragged_plan(np.float32, cuda, tuning="cached")
     assert pl2.tuning() == choice
+
+
+def test_fp64_plans_start_on_lanes_and_refuse_rows(cuda):
+    """The rows sweep runs mixed-precision plans only: an FP64 plan starts with the
+    lanes sweep and refuses rows; a mixed plan starts with 32x16 tiles and rows."""
+    p64 = ragged_plan(np.float64, cuda)
+    assert p64.tuning()[1] == "lanes"
+    with pytest.raises(Exception, match="mixed-precision plans only"):
+        p64.set_tuning("32x8", "rows")
+    assert ragged_plan(np.float32, cuda).tuning() == ("32x16", "rows")
