@@ -112,3 +112,70 @@ def test_repanel_matches_reference():
     for key, kw in REPANEL_KW.items():
         out = repanel(Airfoil(d[f"{key}_in_x"], d[f"{key}_in_y"]), **kw)
         assert np.array_equal(out.x, d[f"{key}_out_x"]) and np.array_equal(out.y, d[f"{key}_out_y"]), key
+
+
+def _fake_plan(lib, precision, B=2):
+    ni = (C.c_int * B)(*([64] * B))
+    nc = (C.c_int * B)(*([24] * B))
+    fake = (C.c_void_p * B)(*([4096] * B))     # never dereferenced before bind
+    winf = (C.c_double * (4 * B))(*([1.0, 0.5, 0.0, 1 / 1.4] * B))
+    p = _lib.default_params()
+    p.precision = precision
+    h = C.c_void_p()
+    _lib.check(lib.a2d_plan_create(B, ni, nc, fake, winf, C.byref(p), C.byref(h)))
+    return h
+
+
+def test_plan_starting_configuration_on_host():
+    """A new mixed plan starts with 32x16 JVP tiles and the rows sweep; an FP64 plan
+    starts on the lanes sweep and refuses rows (host-only: nothing is bound)."""
+    lib = _lib.load()
+    t, v = C.c_int(), C.c_int()
+    hm = _fake_plan(lib, _lib.A2D_MIXED)
+    _lib.check(lib.a2d_plan_get_tuning(hm, C.byref(t), C.byref(v)))
+    assert (t.value, v.value) == (_lib.JVP_TILES["32x16"], _lib.SWEEP_VARIANTS["rows"])
+    h64 = _fake_plan(lib, _lib.A2D_FP64)
+    _lib.check(lib.a2d_plan_get_tuning(h64, C.byref(t), C.byref(v)))
+    assert v.value == _lib.SWEEP_VARIANTS["lanes"]
+    assert lib.a2d_plan_set_tuning(h64, 0, _lib.SWEEP_VARIANTS["rows"], None) == _lib.A2D_ERR_ARG
+    assert b"mixed-precision plans only" in lib.a2d_last_error()
+    _lib.check(lib.a2d_plan_set_tuning(h64, 0, _lib.SWEEP_VARIANTS["pairs"], None))
+    for h in (hm, h64):
+        _lib.check(lib.a2d_plan_destroy(h))
+
+
+def test_service_lanes_layout_on_host():
+    """Slot q of each class goes to lane q mod lanes; the lane count is capped by the
+    largest class; the workspace holds every lane's plan (host-only)."""
+    from aero2d_b200.service import default_lanes
+    lib = _lib.load()
+    ni = (C.c_int * 2)(64, 96)
+    nc = (C.c_int * 2)(24, 32)
+    fake = (C.c_void_p * 2)(4096, 8192)
+    slots = (C.c_int * 2)(5, 2)
+    p = _lib.default_params()
+    p.precision = _lib.A2D_MIXED
+    h = C.c_void_p()
+    _lib.check(lib.a2d_service_create_lanes(2, ni, nc, fake, slots, 3, C.byref(p), C.byref(h)))
+    nl = C.c_int()
+    _lib.check(lib.a2d_service_lanes(h, C.byref(nl)))
+    assert nl.value == 3
+    lanes, total = [], 0
+    for lane in range(3):
+        n = C.c_int()
+        _lib.check(lib.a2d_service_lane(h, lane, None, C.byref(n), None))
+        ids = (C.c_int * n.value)()
+        _lib.check(lib.a2d_service_lane(h, lane, None, None, ids))
+        lanes.append(list(ids))
+    # class 0 owns slots 0..4, class 1 slots 5..6
+    assert lanes == [[0, 3, 5], [1, 4, 6], [2]]
+    ws = C.c_size_t()
+    _lib.check(lib.a2d_service_workspace_bytes(h, C.byref(ws)))
+    assert ws.value > 0
+    _lib.check(lib.a2d_service_destroy(h))
+    h2 = C.c_void_p()
+    _lib.check(lib.a2d_service_create_lanes(2, ni, nc, fake, slots, 8, C.byref(p), C.byref(h2)))
+    _lib.check(lib.a2d_service_lanes(h2, C.byref(nl)))
+    assert nl.value == 5          # at most the largest class's slot count
+    _lib.check(lib.a2d_service_destroy(h2))
+    assert [default_lanes(c) for c in ([64], [16], [8], [32], [394, 176, 99, 44])] == [4, 1, 1, 2, 4]
