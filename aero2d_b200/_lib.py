@@ -22,7 +22,7 @@ A2D_MIXED = 1
 
 # tuning knobs (a2d_plan_set_tuning)
 JVP_TILES = {"32x8": 0, "32x16": 1, "64x4": 2, "16x16": 3}
-SWEEP_VARIANTS = {"lanes": 0, "rows": 1, "pairs": 2}
+SWEEP_VARIANTS = {"lanes": 0, "rows": 1, "pairs": 2, "halves": 3}
 
 VEC_U, VEC_R, VEC_V, VEC_JV, VEC_DU = 0, 1, 2, 3, 4
 

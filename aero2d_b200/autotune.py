@@ -35,8 +35,9 @@ from pathlib import Path
 from typing import Callable, Iterable, Optional
 
 JVP_TILES = ("32x8", "32x16", "64x4", "16x16")
-SWEEPS = ("lanes", "rows", "pairs")
-DEFAULT = ("32x16", "rows")   # a new plan's configuration (the library's defaults)
+SWEEPS = ("lanes", "rows", "pairs", "halves")
+MIXED_ONLY_SWEEPS = ("rows", "halves")   # refused on FP64 plans
+DEFAULT = ("32x16", "halves")   # a new plan's configuration (the library's defaults)
 
 
 def default_path() -> Path:
@@ -64,10 +65,10 @@ def signature(shapes: Iterable[tuple[int, int]], precision: int) -> str:
 def candidates(precision: int) -> list[tuple[str, str]]:
     """Every configuration worth timing: the JVP tile shapes matter only in
     the mixed precision (the FP64 JVP always runs 32 x 8 tiles), and the rows
-    sweep runs mixed-precision plans only."""
+    and halves sweeps run mixed-precision plans only."""
     if precision:
         return [(t, v) for t in JVP_TILES for v in SWEEPS]
-    return [(JVP_TILES[0], v) for v in SWEEPS if v != "rows"]
+    return [(JVP_TILES[0], v) for v in SWEEPS if v not in MIXED_ONLY_SWEEPS]
 
 
 class TuningCache:

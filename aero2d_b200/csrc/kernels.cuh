@@ -123,10 +123,10 @@ void launch_factor(const Batch& b, const FactorArgs& a, cudaStream_t s);
 // half line group: one, a lane solving all four block rows of its line
 // (sweep.cu); two, two lanes per line with two block rows each (sweep_pairs.cu);
 // four, a warp per block row (sweep_rows.cu)
-enum : int { kSweepLanes = 0, kSweepRows = 1, kSweepPairs = 2, kNumSweepVariants = 3 };
+enum : int { kSweepLanes = 0, kSweepRows = 1, kSweepPairs = 2, kSweepHalves = 3, kNumSweepVariants = 4 };
 
 // one line-Jacobi sweep; FIRST: the sweep without i-coupling; last: x is the
-// FP64 result (else an intermediate vector).  Both variants compute the same
+// FP64 result (else an intermediate vector).  Every variant computes the same
 // arithmetic in the same order
 template <typename TI, bool FIRST>
 void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s, int variant = kSweepLanes);
@@ -134,10 +134,13 @@ template <typename TI, bool FIRST>
 void launch_sweep_rows(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s);
 template <typename TI, bool FIRST>
 void launch_sweep_pairs(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s);
+template <bool FIRST>   // mixed precision only
+void launch_sweep_halves(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s);
 
 // raises the dynamic shared-memory limit of the sweep kernels (host, once per device)
 cudaError_t sweep_init();
 cudaError_t sweep_rows_init();
 cudaError_t sweep_pairs_init();
+cudaError_t sweep_halves_init();
 
 }  // namespace a2d

@@ -77,11 +77,11 @@ struct a2d_plan {
   std::vector<CaseDev> cases;
   std::vector<Tile> tiles;
   std::vector<Tile> jtiles;    // tiles of the FP32 linearised stencil, in the shape jvp_tile
-  // tuning knobs (a2d_plan_set_tuning); the defaults are the autotuner's choice on every
-  // batch shape measured on a B200 (64 and 4 x 16 cases of 256 x 64, the ragged sets); FP64
-  // plans start with the lanes sweep
+  // tuning knobs (a2d_plan_set_tuning); the defaults are the fastest measured on a B200 on
+  // the batch shapes timed (64, 4 x 16 and 8 cases of 256 x 64); FP64 plans start with the
+  // lanes sweep
   int jvp_tile = kTile32x16;
-  int sweep_variant = kSweepRows;
+  int sweep_variant = kSweepHalves;
   int max_jtiles = 0;          // the most tiles any JVP tile shape needs (workspace room)
   std::vector<Chunk> chunks;
   std::vector<Group> groups;
@@ -760,8 +760,8 @@ int a2d_plan_set_tuning(a2d_plan* P, int jvp_tile, int sweep_variant, void* stre
   if (jvp_tile < 0 || jvp_tile >= kNumTileShapes) return fail(A2D_ERR_ARG, "set_tuning: unknown JVP tile shape");
   if (sweep_variant < 0 || sweep_variant >= kNumSweepVariants)
     return fail(A2D_ERR_ARG, "set_tuning: unknown sweep variant");
-  if (sweep_variant == kSweepRows && P->p.precision != A2D_MIXED)
-    return fail(A2D_ERR_ARG, "set_tuning: the rows sweep runs mixed-precision plans only");
+  if ((sweep_variant == kSweepRows || sweep_variant == kSweepHalves) && P->p.precision != A2D_MIXED)
+    return fail(A2D_ERR_ARG, "set_tuning: the rows and halves sweeps run mixed-precision plans only");
   if (jvp_tile != P->jvp_tile) {
     P->jvp_tile = jvp_tile;
     P->jtiles = tile_list(P, jvp_tile);

@@ -452,9 +452,13 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Batch b, SweepArgs a) {
 template <typename TI, bool FIRST>
 void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s, int variant) {
   if (b.ngroups == 0) return;
-  if constexpr (sizeof(TI) == 4) {   // the rows variant runs mixed-precision plans only
+  if constexpr (sizeof(TI) == 4) {   // the rows and halves variants run mixed-precision plans only
     if (variant == kSweepRows) {
       launch_sweep_rows<TI, FIRST>(b, a, last, s);
+      return;
+    }
+    if (variant == kSweepHalves) {
+      launch_sweep_halves<FIRST>(b, a, last, s);
       return;
     }
   }
@@ -469,6 +473,7 @@ void launch_sweep(const Batch& b, const SweepArgs& a, bool last, cudaStream_t s,
 cudaError_t sweep_init() {
   cudaError_t e = sweep_rows_init();
   if (e == cudaSuccess) e = sweep_pairs_init();
+  if (e == cudaSuccess) e = sweep_halves_init();
   auto set = [&](const void* f, size_t bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   };

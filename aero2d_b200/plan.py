@@ -75,7 +75,7 @@ class Plan:
     default) applies the autotuner's stored choice for this plan's grid sizes
     and precision if there is one; "auto" also measures and stores it when there
     is none; None keeps the library's starting configuration (32x16 JVP tiles and
-    the rows sweep; FP64 plans the lanes sweep); a (jvp_tile, sweep) pair sets it.
+    the halves sweep; FP64 plans the lanes sweep); a (jvp_tile, sweep) pair sets it.
     Results do not depend on it."""
 
     def __init__(self, grids: list[DeviceGrid], winf: np.ndarray, params: _lib.Params, device=None,
@@ -111,7 +111,7 @@ class Plan:
     def shapes(self) -> list[tuple[int, int]]:
         return [(g.ni, g.nc) for g in self.grids]
 
-    def set_tuning(self, jvp_tile: str = "32x16", sweep: str = "rows") -> None:
+    def set_tuning(self, jvp_tile: str = "32x16", sweep: str = "halves") -> None:
         """The launch configuration: the FP32 JVP's tile shape and the line
         sweep's kernel variant (include/aero2d_b200.h, A2D_JVP_TILE_*, A2D_SWEEP_*)."""
         with torch.cuda.device(self.device):

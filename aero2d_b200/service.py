@@ -273,7 +273,7 @@ class _PlanView:
             for h in self.handles:
                 _lib.check(getattr(self.lib, name)(h, *args, stream_handle(self.device)))
 
-    def set_tuning(self, jvp_tile: str = "32x16", sweep: str = "rows") -> None:
+    def set_tuning(self, jvp_tile: str = "32x16", sweep: str = "halves") -> None:
         self._each("a2d_plan_set_tuning", _lib.JVP_TILES[jvp_tile], _lib.SWEEP_VARIANTS[sweep])
 
     def tuning(self) -> tuple[str, str]:

@@ -109,8 +109,11 @@ int a2d_plan_ncases(const a2d_plan* plan);
 #define A2D_SWEEP_LANES 0       /* line sweep: one warp per half line group, a lane per line   */
 #define A2D_SWEEP_ROWS 1        /* line sweep: four warps per half line group, a warp per block row */
 #define A2D_SWEEP_PAIRS 2       /* line sweep: two warps per half line group, two lanes per line */
-/* a new plan starts with A2D_JVP_TILE_32x16 and A2D_SWEEP_ROWS (FP64 plans: A2D_SWEEP_LANES);
- * A2D_SWEEP_ROWS is refused on FP64 plans (A2D_ERR_ARG) */
+#define A2D_SWEEP_HALVES 3      /* line sweep: a cluster of two CTAs per line group, one per half,  */
+                                /* a warp per block row, the halves meeting in distributed shared  */
+                                /* memory                                                           */
+/* a new plan starts with A2D_JVP_TILE_32x16 and A2D_SWEEP_HALVES (FP64 plans: A2D_SWEEP_LANES);
+ * A2D_SWEEP_ROWS and A2D_SWEEP_HALVES are refused on FP64 plans (A2D_ERR_ARG) */
 /* any time, bound or not; a change re-captures the Newton step's graph at the next step */
 int a2d_plan_set_tuning(a2d_plan* plan, int jvp_tile, int sweep_variant, void* stream);
 int a2d_plan_get_tuning(const a2d_plan* plan, int* jvp_tile, int* sweep_variant);

@@ -19,7 +19,7 @@ def test_candidates_by_precision():
     mixed = autotune.candidates(1)
     assert len(mixed) == len(autotune.JVP_TILES) * len(autotune.SWEEPS)
     assert set(t for t, _ in autotune.candidates(0)) == {"32x8"}
-    assert "rows" not in set(v for _, v in autotune.candidates(0))   # the rows sweep is mixed-only
+    assert not set(v for _, v in autotune.candidates(0)) & set(autotune.MIXED_ONLY_SWEEPS)
     assert autotune.DEFAULT in mixed
 
 

@@ -56,10 +56,12 @@ def test_autotuner_measures_stores_and_reapplies(cuda, tmp_path, monkeypatch):
 
 
 def test_fp64_plans_start_on_lanes_and_refuse_rows(cuda):
-    """The rows sweep runs mixed-precision plans only: an FP64 plan starts with the
-    lanes sweep and refuses rows; a mixed plan starts with 32x16 tiles and rows."""
+    """The rows and halves sweeps run mixed-precision plans only: an FP64 plan starts
+    with the lanes sweep and refuses them; a mixed plan starts with 32x16 tiles and
+    the halves sweep."""
     p64 = ragged_plan(np.float64, cuda)
     assert p64.tuning()[1] == "lanes"
-    with pytest.raises(Exception, match="mixed-precision plans only"):
-        p64.set_tuning("32x8", "rows")
-    assert ragged_plan(np.float32, cuda).tuning() == ("32x16", "rows")
+    for v in ("rows", "halves"):
+        with pytest.raises(Exception, match="mixed-precision plans only"):
+            p64.set_tuning("32x8", v)
+    assert ragged_plan(np.float32, cuda).tuning() == ("32x16", "halves")

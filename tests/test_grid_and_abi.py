@@ -127,18 +127,19 @@ def _fake_plan(lib, precision, B=2):
 
 
 def test_plan_starting_configuration_on_host():
-    """A new mixed plan starts with 32x16 JVP tiles and the rows sweep; an FP64 plan
-    starts on the lanes sweep and refuses rows (host-only: nothing is bound)."""
+    """A new mixed plan starts with 32x16 JVP tiles and the halves sweep; an FP64 plan
+    starts on the lanes sweep and refuses rows and halves (host-only: nothing is bound)."""
     lib = _lib.load()
     t, v = C.c_int(), C.c_int()
     hm = _fake_plan(lib, _lib.A2D_MIXED)
     _lib.check(lib.a2d_plan_get_tuning(hm, C.byref(t), C.byref(v)))
-    assert (t.value, v.value) == (_lib.JVP_TILES["32x16"], _lib.SWEEP_VARIANTS["rows"])
+    assert (t.value, v.value) == (_lib.JVP_TILES["32x16"], _lib.SWEEP_VARIANTS["halves"])
     h64 = _fake_plan(lib, _lib.A2D_FP64)
     _lib.check(lib.a2d_plan_get_tuning(h64, C.byref(t), C.byref(v)))
     assert v.value == _lib.SWEEP_VARIANTS["lanes"]
-    assert lib.a2d_plan_set_tuning(h64, 0, _lib.SWEEP_VARIANTS["rows"], None) == _lib.A2D_ERR_ARG
-    assert b"mixed-precision plans only" in lib.a2d_last_error()
+    for v in ("rows", "halves"):
+        assert lib.a2d_plan_set_tuning(h64, 0, _lib.SWEEP_VARIANTS[v], None) == _lib.A2D_ERR_ARG
+        assert b"mixed-precision plans only" in lib.a2d_last_error()
     _lib.check(lib.a2d_plan_set_tuning(h64, 0, _lib.SWEEP_VARIANTS["pairs"], None))
     for h in (hm, h64):
         _lib.check(lib.a2d_plan_destroy(h))
