@@ -6,7 +6,10 @@
 // 512 CTAs of nine warps sit four on some SMs and three on others and the launch
 // lasts as long as the SMs holding four.  In each CTA warps 0-3 are the block rows
 // q (lane = line) and warp 4 the producer streaming the half's factor blocks by
-// bulk copies into a ring of full/empty mbarriers, as in the rows variant.  The
+// bulk copies into a ring of full/empty mbarriers, as in the rows variant, except
+// that the back substitution takes four steps per ring stage: its steps read one C
+// block each (1 KB of a 4 KB stage), and the rows of four consecutive steps are
+// consecutive, so one bulk copy brings a pack and the ring holds 16 back steps.  The
 // halves meet twice, through distributed shared memory: the far-field CTA stores
 // its last forward vector d'_{k+1} into the wall CTA's shared memory and arrives
 // on an mbarrier there; the wall CTA solves the twist row and stores x_k into the
@@ -35,6 +38,8 @@ constexpr int kBlockEntries = 16 * kLanes;              // one 4x4 block for the
 constexpr int kBackAhead = 8;                           // register prefetch depth of d in the back substitution
 constexpr int kStages = 4;                              // bulk-copy ring stages
 constexpr int kAhead = 4;                               // steps between loading a vector entry and its use
+constexpr int kPack = 4;                                // back-substitution steps per ring stage (their rows are contiguous)
+static_assert(kBackAhead % kPack == 0, "a back prefetch block holds whole packs");
 
 struct SweepSmem {
   static constexpr uint32_t kBytesI = kBlockEntries * sizeof(TI);
@@ -166,6 +171,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSweepThreads, 7) k_
   const int nf0 = k, nf1 = nc - 1 - k;         // forward steps of the wall / far-field half
   const int nf = h == 0 ? nf0 : nf1;
   const int nsteps = h == 0 ? 2 * k + 1 : 2 * nf1;   // this half's steps
+  const int tb0 = h == 0 ? k + 1 : nf1;              // this half's first back-substitution step
+  const int nslots = tb0 + (nsteps - tb0 + kPack - 1) / kPack;   // ring slots: one per forward step, one per pack
   // step t of the half: forward rows first; the wall half's step k is the twist
   // row; then the back substitution outward from the twist row
   auto row_of = [&](int t) {
@@ -202,20 +209,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSweepThreads, 7) k_
     int issued = 0;
     bool ok = true;
 #pragma unroll 1
-    for (int t = 0; t < nsteps && ok; ++t) {
-      const int s = t % S;
-      if (t >= S && !mbar_wait(&sm.empty[s], ((t / S) - 1) & 1)) {
+    for (int n = 0; n < nslots && ok; ++n) {
+      const int s = n % S;
+      if (n >= S && !mbar_wait(&sm.empty[s], ((n / S) - 1) & 1)) {
         ok = false;
         break;
       }
-      const int j = row_of(t);
+      const bool fwd = n < tb0;                  // forward steps and the twist: one step per slot
+      const int t = fwd ? n : tb0 + (n - tb0) * kPack;
       const bool twist = h == 0 && t == k;
-      const bool fwd = twist || t < nf;
       uint64_t* bar = &sm.full[s];
       if (lane == 0) {
         unsigned char* m = sm.mat[s];
-        const size_t o = blk0 + (size_t)j * kBlockEntries;
         if (fwd) {
+          const size_t o = blk0 + (size_t)row_of(t) * kBlockEntries;
           if constexpr (FIRST) {
             mbar_arrive_expect(bar, kBytesI + (twist ? 2 : 1) * kBytesF);
             bulk_load_hint(m, INV + o, kBytesI, bar, pol);
@@ -227,11 +234,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSweepThreads, 7) k_
             if (twist) bulk_load_hint(m + kOffH, CF + o, kBytesF, bar, pol);
           }
         } else {
-          mbar_arrive_expect(bar, kBytesF);
-          bulk_load_hint(m, CF + o, kBytesF, bar, pol);
+          // a pack of up to kPack back steps: their rows are consecutive, so their C
+          // blocks are one run starting at the lowest row
+          const int c = min(kPack, nsteps - t);
+          const int jlo = h == 0 ? row_of(t + c - 1) : row_of(t);
+          const size_t o = blk0 + (size_t)jlo * kBlockEntries;
+          mbar_arrive_expect(bar, c * kBytesF);
+          bulk_load_hint(m, CF + o, c * kBytesF, bar, pol);
         }
       }
-      issued = t + 1;
+      issued = n + 1;
     }
     if (!ok) {
       // the consumers stopped: record it, and give the copies still in flight
@@ -427,6 +439,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSweepThreads, 7) k_
     int boff = (h == 0 ? k - 1 : k + 1) * ni;   // row of back step t0
     int poff = boff;                            // row of the next prefetch
     TC dbuf[kBackAhead];
+    int pslot = 0;                              // wall half: the pack's first step's block in the stage
 #pragma unroll
     for (int u = 0; u < kBackAhead; ++u) {
       dbuf[u] = t0 + u < nsteps ? dvb[poff] : TC(0);
@@ -438,12 +451,22 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSweepThreads, 7) k_
       for (int u = 0; u < kBackAhead; ++u) {
         const int t = b0 + u;
         if (t < nsteps && tstop < 0) {
-          const int s = t % S;
-          wait_full(t);
+          // t - t0 = (b0 - t0) + u with b0 - t0 a multiple of kPack: the step's place
+          // in its pack is u % kPack, known at compile time
+          const int n = tb0 + (t - tb0) / kPack;   // ring slot of the pack
+          const int s = n % S;
+          if (u % kPack == 0) {
+            wait_full(n);
+            // the pack's run starts at its lowest row: the wall half walks down
+            const int c = min(kPack, nsteps - (t - u % kPack));
+            pslot = h == 0 ? c - 1 : 0;
+          }
           TC cv[4], xn[4];
-          load4(reinterpret_cast<const TF*>(sm.mat[s]) + eo, cv);
-          release(t);
-          ++done;
+          load4(reinterpret_cast<const TF*>(sm.mat[s] + (h == 0 ? pslot - u % kPack : u % kPack) * kBytesF) + eo, cv);
+          if (u % kPack == kPack - 1 || t + 1 == nsteps) {
+            release(n);
+            ++done;
+          }
           load4(t == t0 ? &sm.xk[l][0] : &sm.xchg[(t + 1) & 1][l][0], xn);
           TC acc = cv[0] * xn[0];
 #pragma unroll
@@ -465,7 +488,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSweepThreads, 7) k_
     // bounded time to land
     if (a.err != nullptr) atomicExch(a.err, 1u);
 #pragma unroll 1
-    for (int u = done > 0 ? done - 1 : 0; u < done + S && u < nsteps; ++u) (void)mbar_wait(&sm.full[u % S], (u / S) & 1);
+    for (int u = done > 0 ? done - 1 : 0; u < done + S && u < nslots; ++u) (void)mbar_wait(&sm.full[u % S], (u / S) & 1);
   }
   cluster_sync();   // neither CTA leaves while the other may still store into its shared memory
 }

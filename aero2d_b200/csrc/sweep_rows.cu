@@ -5,7 +5,8 @@
 // line's 4-vector passes between the four row warps of a half through a two-slot
 // shared exchange buffer, one named barrier per step); warp 8 is the producer:
 // for every step of each half its lane 0 brings the step's blocks by TMA bulk
-// copies into a ring of kStages stages per half with two mbarriers per stage,
+// copies (the back substitution's C blocks four consecutive rows to a copy) into
+// a ring of kStages stages per half with two mbarriers per stage,
 // "full" (the bulk-copy bytes) and "empty" (one arrival per consumer warp done
 // with the stage).  Each consumer thread loads its own vector entries of the
 // forward steps (component q of its line) through L2 into registers kAhead
@@ -34,6 +35,8 @@ constexpr int kProducerWarp = kConsumerThreads / 32;    // warp 8
 constexpr int kSweepThreads = kConsumerThreads + 32;
 constexpr int kBlockEntries = 16 * kLanes;              // one 4x4 block for the 32 lines of a group
 constexpr int kBackAhead = 8;                           // register prefetch depth of d in the back substitution
+constexpr int kPack = 4;                                // back-substitution steps per ring stage (their rows are contiguous)
+static_assert(kBackAhead % kPack == 0, "a back prefetch block holds whole packs");
 
 // TI: pivot inverses (the Jacobian type); TF: the other factors (FactorStore);
 // TC: arithmetic and intermediate vectors
@@ -130,6 +133,10 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   const int k = nc / 2;                        // twist row (as in k_factor)
   const int nf0 = k, nf1 = nc - 1 - k;         // forward steps of the wall / far-field half
   const int ns0 = 2 * k + 1, ns1 = 2 * nf1;    // steps of each half
+  // ring slots of each half: one per forward step (and the twist), then one per
+  // pack of up to kPack back-substitution steps, from the half's first back step
+  const int nsl0 = k + 1 + (ns0 - k - 1 + kPack - 1) / kPack;
+  const int nsl1 = nf1 + (ns1 - nf1 + kPack - 1) / kPack;
   // step t of half h: forward rows first; the wall half's step k is the twist
   // row; then the back substitution outward from the twist row
   auto row_of = [&](int h, int t) {
@@ -167,25 +174,26 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     const uint64_t pol = l2_evict_first();   // factor blocks are read once per sweep
     int issued[2] = {0, 0};
     bool ok = true;
-    const int smax = ns0 > ns1 ? ns0 : ns1;
+    const int nmax = nsl0 > nsl1 ? nsl0 : nsl1;
 #pragma unroll 1
-    for (int t = 0; t < smax && ok; ++t) {
+    for (int n = 0; n < nmax && ok; ++n) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        if (!ok || t >= (h == 0 ? ns0 : ns1)) continue;
-        const int s = t % S;
-        if (t >= S && !mbar_wait(&sm.empty[h][s], ((t / S) - 1) & 1)) {
+        if (!ok || n >= (h == 0 ? nsl0 : nsl1)) continue;
+        const int s = n % S;
+        if (n >= S && !mbar_wait(&sm.empty[h][s], ((n / S) - 1) & 1)) {
           ok = false;
           continue;
         }
-        const int j = row_of(h, t);
+        const int tb = h == 0 ? k + 1 : nf1;      // the half's first back step
+        const bool fwd = n < tb;                  // forward steps and the twist: one step per slot
+        const int t = fwd ? n : tb + (n - tb) * kPack;
         const bool twist = h == 0 && t == k;
-        const bool fwd = twist || t < (h == 0 ? nf0 : nf1);
         uint64_t* bar = &sm.full[h][s];
         if (lane == 0) {
           unsigned char* m = sm.mat[h][s];
-          const size_t o = blk0 + (size_t)j * kBlockEntries;
           if (fwd) {
+            const size_t o = blk0 + (size_t)row_of(h, t) * kBlockEntries;
             if constexpr (FIRST) {
               mbar_arrive_expect(bar, kBytesI + (twist ? 2 : 1) * kBytesF);
               bulk_load_hint(m, INV + o, kBytesI, bar, pol);
@@ -197,11 +205,16 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
               if (twist) bulk_load_hint(m + kOffH, CF + o, kBytesF, bar, pol);
             }
           } else {
-            mbar_arrive_expect(bar, kBytesF);
-            bulk_load_hint(m, CF + o, kBytesF, bar, pol);
+            // a pack of up to kPack back steps: their rows are consecutive, so
+            // their C blocks are one run starting at the lowest row
+            const int c = min(kPack, (h == 0 ? ns0 : ns1) - t);
+            const int jlo = h == 0 ? row_of(h, t + c - 1) : row_of(h, t);
+            const size_t o = blk0 + (size_t)jlo * kBlockEntries;
+            mbar_arrive_expect(bar, c * kBytesF);
+            bulk_load_hint(m, CF + o, c * kBytesF, bar, pol);
           }
         }
-        issued[h] = t + 1;
+        issued[h] = n + 1;
       }
     }
     if (!ok) {
@@ -399,6 +412,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
     int boff = (h == 0 ? k - 1 : k + 1) * ni;               // row of back step t0
     int poff = boff;                                        // row of the next prefetch
     TC dbuf[kBackAhead];
+    int pslot = 0;                                          // wall half: the pack's first step's block in the stage
 #pragma unroll
     for (int u = 0; u < kBackAhead; ++u) {
       dbuf[u] = t0 + u < nsteps ? dvb[poff] : TC(0);
@@ -410,11 +424,18 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
       for (int u = 0; u < kBackAhead; ++u) {
         const int t = b0 + u;
         if (t < nsteps && tstop < 0) {
-          const int s = t % S;
-          wait_full(t);
+          // b0 - t0 is a multiple of kPack: the step's place in its pack is u % kPack
+          const int n = t0 + (t - t0) / kPack;     // ring slot of the pack
+          const int s = n % S;
+          if (u % kPack == 0) {
+            wait_full(n);
+            // the pack's run starts at its lowest row: the wall half walks down
+            const int c = min(kPack, nsteps - (t - u % kPack));
+            pslot = h == 0 ? c - 1 : 0;
+          }
           TC cv[4], xn[4];
-          load4(reinterpret_cast<const TF*>(sm.mat[h][s]) + eo, cv);
-          release(t);
+          load4(reinterpret_cast<const TF*>(sm.mat[h][s] + (h == 0 ? pslot - u % kPack : u % kPack) * kBytesF) + eo, cv);
+          if (u % kPack == kPack - 1 || t + 1 == nsteps) release(n);
           load4(t == t0 ? &sm.xk[l][0] : &sm.xchg[h][(t + 1) & 1][l][0], xn);
           TC acc = cv[0] * xn[0];
 #pragma unroll
@@ -432,10 +453,12 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_sweep(Batch b, SweepArgs a
   }
   if (tstop >= 0 && l == 0 && q == 0) {
     // a copy never landed: record it, and give the copies that may still be in
-    // flight for this half (issued for steps tstop .. tstop+S-1) a bounded time
+    // flight for this half (issued for ring slots n .. n+S-1 from the slot of step
+    // tstop) a bounded time
     if (a.err != nullptr) atomicExch(a.err, 1u);
+    const int n0 = tstop < t0 ? tstop : t0 + (tstop - t0) / kPack;
 #pragma unroll 1
-    for (int u = tstop; u < tstop + S && u < nsteps; ++u) (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
+    for (int u = n0; u < n0 + S && u < (h == 0 ? nsl0 : nsl1); ++u) (void)mbar_wait(&sm.full[h][u % S], (u / S) & 1);
   }
 }
 
