@@ -1,6 +1,6 @@
 """The launch-configuration knobs on the GPU: every (JVP tile shape, sweep
 variant) takes bitwise the same Newton step, in FP64 and mixed precision, on a
-ragged batch (two grid sizes); the autotuner measures, stores and re-applies a
+ragged batch (three grid sizes); the autotuner measures, stores and re-applies a
 choice through its cache."""
 import numpy as np
 import pytest
@@ -16,11 +16,14 @@ pytestmark = pytest.mark.gpu
 
 
 def ragged_plan(dtype, cuda, tuning=None):
-    ga, gb = grid("2412", 65, 33), grid("0012", 49, 25)
-    sa, sb = EulerSolver(ga, dtype=dtype, device=cuda), EulerSolver(gb, dtype=dtype, device=cuda)
+    # 128 x 32, 96 x 24 and 80 x 42 cells: the last has a half-full line group and a
+    # twist row (21) whose wall-side back substitution ends on a short pack of the
+    # sweeps' ring (packs of four C blocks); the others end short on the far-field side
+    ga, gb, gc = grid("2412", 65, 33), grid("0012", 49, 25), grid("4412", 41, 43)
+    sa, sb, sc = (EulerSolver(g, dtype=dtype, device=cuda) for g in (ga, gb, gc))
     imp = ImplicitEuler(sa, gmres_restart=20)
-    machs, alphas = np.array([0.5, 0.7, 0.6]), np.array([2.0, 1.0, -1.0])
-    return Plan([sa.dgrid, sb.dgrid, sa.dgrid], sa.freestream(machs, alphas), imp.params(1e-10, 20), cuda,
+    machs, alphas = np.array([0.5, 0.7, 0.6, 0.55]), np.array([2.0, 1.0, -1.0, 3.0])
+    return Plan([sa.dgrid, sb.dgrid, sa.dgrid, sc.dgrid], sa.freestream(machs, alphas), imp.params(1e-10, 20), cuda,
                 tuning=tuning)
 
 
