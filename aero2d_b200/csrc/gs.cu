@@ -152,7 +152,9 @@ __device__ __forceinline__ void stv(__nv_bfloat16* p, const double (&v)[4]) {
 // sub-tiles of E entries; the E entries of w and of every basis vector of the
 // slice for one sub-tile (one stage) arrive by bulk copies on one mbarrier,
 // through a ring of as many stages as the shared-memory budget holds, issued
-// by thread 0 as soon as a stage is free.  Thread t works on entries
+// by thread 0 as soon as a stage is free.  The BF16 basis takes a smaller budget
+// than the others, so that more CTAs fit on an SM (measured at 64 cases: resident
+// CTAs hide the bulk copies better than a deeper ring).  Thread t works on entries
 // t*EPT .. t*EPT+EPT-1 of each sub-tile and keeps one partial sum per basis
 // vector in registers (NQ >= nq of them, a template tier); the chunk ends with
 // one fixed-order block reduction, so the result does not depend on which
@@ -179,9 +181,16 @@ static_assert(kGsSmemBudget >= (size_t)GsTile<float>::E * (32 * 4 + 8) &&
                   kGsSmemBudget >= (size_t)GsTile<__nv_bfloat16>::E * (32 * 2 + 8),
               "one stage of a 32-vector slice must fit the shared-memory budget");
 
+// shared-memory budget of the ring: 40 KB for the BF16 basis (slices of up to 13
+// vectors keep 2 stages or more, larger ones one stage and four or five CTAs per SM)
+template <typename TB>
+__host__ __device__ constexpr size_t gs_budget() {
+  return std::is_same<TB, __nv_bfloat16>::value ? 40 * 1024 : kGsSmemBudget;
+}
+
 template <typename TB>
 __host__ __device__ inline int gs_stages(int nq) {
-  const int s = (int)(kGsSmemBudget / gs_stage_bytes<TB>(nq));
+  const int s = (int)(gs_budget<TB>() / gs_stage_bytes<TB>(nq));
   return s < 1 ? 1 : (s > kGsMaxStages ? kGsMaxStages : s);
 }
 
@@ -357,7 +366,8 @@ __global__ void __launch_bounds__(kGT) k_gs_dots(Batch b, GsArgs<TB> a) {
 
 // pass 2, fused: w' = w - V (s h1), then V . w' --------------------------------
 template <typename TB, int NQ>
-__global__ void __launch_bounds__(kGT) k_gs_project(Batch b, GsArgs<TB> a) {
+__global__ void __launch_bounds__(kGT, (NQ == 24 && std::is_same<TB, __nv_bfloat16>::value) ? 3 : 0)
+    k_gs_project(Batch b, GsArgs<TB> a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double coef[NQ];
   const Chunk ch = b.chunks[blockIdx.x];
